@@ -1,0 +1,425 @@
+#!/usr/bin/env python3
+"""Benchmark of the batched small-GEMM path on B200.
+
+Workload (one "step"): the cube sweep M = N = K in {8, 16, ..., 128} in both
+NN (B is K x N) and NT (B is N x K) layouts, each a uniform batch of 10,000
+independent FP32 GEMMs, C = A op(B), row-major, inputs uniform in [-1, 1).
+That is 32 calls of LibShalom_sgemm_batched_strided per step: 379.3 GFLOP and
+22.98 GB of algorithmic HBM traffic (A and B read, C written, 4 bytes each).
+
+  value    whole-job GFLOP/s with inputs resident in HBM (device-timed)
+  e2e      the same through the C ABI with the inputs in pinned HOST memory:
+           every step copies A and B in and C out (copies inside the timed
+           region)
+  roofline the dominant kernel's algorithmic bytes / its CUDA-event time,
+           against the measured HBM copy bandwidth
+  cpu_baseline the reference's algorithm restated in C (the reference is
+           AArch64 NEON assembly and cannot run on this x86 host), OpenMP
+           over the batch, on a bounded sample of the same workload
+
+`--impl reference` times only that CPU restatement (all host threads) and
+prints its own line.  Under torchrun each rank runs an independent replica
+(the batch shards by GEMM index; no data-path collective); rank 0 prints.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+SIZES = list(range(8, 129, 8))
+LAYOUTS = (0, 1)  # NoTrans (NN), Trans (NT)
+BATCH = 10_000
+METRIC = "batched small-GEMM GFLOP/s (cube sweep 8..128, NN+NT, 10,000 per size)"
+
+
+def step_flops(batch=BATCH):
+    return sum(2.0 * n ** 3 * batch for n in SIZES for _ in LAYOUTS)
+
+
+def step_bytes(batch=BATCH):
+    return sum(4.0 * 3 * n * n * batch for n in SIZES for _ in LAYOUTS)
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=5)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    p.add_argument("--mode", default="auto", choices=["auto", "fp32", "bf16x3", "bf16x6"])
+    p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--no-cpu", action="store_true")
+    return p.parse_args()
+
+
+def dist_env():
+    return (int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")),
+            int(os.environ.get("LOCAL_RANK", "0")))
+
+
+# --------------------------------------------------------------------------
+# CPU restatement of the reference (cpu_baseline leg and --impl reference)
+# --------------------------------------------------------------------------
+
+def cpu_sample(seconds_target=12.0, threads=None):
+    """Times the oracle's port of the reference algorithm on a bounded sample
+    of the sweep (cpu_sample_batch GEMMs per size and layout, all host
+    threads).  Returns (GFLOP/s, cores, description)."""
+    from oracle import oracle as orc
+    threads = threads or orc.max_threads()
+    per = 64
+    # calibrate on a small pass, then size the sample for ~seconds_target
+    dt = _cpu_pass(orc, per, threads)
+    per = int(max(per, min(BATCH, per * seconds_target / max(dt, 1e-3))))
+    dt = _cpu_pass(orc, per, threads)
+    return step_flops(per) / dt / 1e9, threads, per, dt
+
+
+_CPU_INPUTS = {}
+
+
+def _cpu_inputs(per):
+    if per not in _CPU_INPUTS:
+        _CPU_INPUTS.clear()
+        rng = np.random.default_rng(0)
+        _CPU_INPUTS[per] = [((rng.random(per * n * n, dtype=np.float32) * 2 - 1),
+                             (rng.random(per * n * n, dtype=np.float32) * 2 - 1),
+                             np.empty(per * n * n, np.float32)) for n in SIZES]
+    return _CPU_INPUTS[per]
+
+
+def _cpu_pass(orc, per, threads):
+    """One pass of the sweep on the CPU; returns the compute seconds (input
+    generation excluded)."""
+    bufs = _cpu_inputs(per)
+    t0 = time.perf_counter()
+    for n, (A, B, C) in zip(SIZES, bufs):
+        for tb in LAYOUTS:
+            orc.port_sgemm_strided(tb, n, n, n, per, A, B, C, threads)
+    return time.perf_counter() - t0
+
+
+def cpu_info():
+    model = ""
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                model = line.split(":", 1)[1].strip()
+                break
+    except OSError:
+        pass
+    return model, os.cpu_count()
+
+
+def run_reference(args):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return 0
+    from oracle import oracle as orc
+    threads = orc.max_threads()
+    # each step is a bounded sample of the sweep, sized so the run stays short
+    per = 256
+    times = []
+    for i in range(args.warmup + args.steps):
+        dt = _cpu_pass(orc, per, threads)
+        if i >= args.warmup:
+            times.append(dt)
+    t = float(np.mean(times))
+    value = step_flops(per) / t / 1e9
+    model, ncpu = cpu_info()
+    sample = (f"cube sweep 8..128 NN+NT, {per} GEMMs per size and layout per step "
+              f"({step_flops(per) / 1e9:.2f} GFLOP), C restatement of the reference's "
+              f"5x16 register-tile algorithm (AArch64 NEON assembly not buildable on x86), "
+              f"OpenMP over GEMMs, {threads} threads on {model}")
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "GFLOP/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": t * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": "cube sweep 8..128 NN+NT, uniform batches", "batch_per_size": per,
+                   "host_cpu": model, "host_threads": threads},
+        "cpu_baseline": {"value": value, "unit": "GFLOP/s", "cores": threads, "kind": "port",
+                         "sample": sample},
+        "e2e": {"value": value, "unit": "GFLOP/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# --------------------------------------------------------------------------
+# GPU arm
+# --------------------------------------------------------------------------
+
+class Clocks:
+    """nvidia-smi sampling during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            out, _ = self.proc.communicate(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+            out, _ = self.proc.communicate()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in out.strip().splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        # median under load: samples at or above half the max clock
+        load = [s for s in sm if smax and s >= 0.5 * smax] or sm
+        return {"sm_mhz": float(np.median(load)) if load else None, "sm_max_mhz": smax,
+                "samples": len(sm), "reasons": sorted(reasons)}
+
+
+def run_gpu(args):
+    import torch
+    rank, world, local = dist_env()
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    import libshalom_b200 as ls
+
+    mode = {"auto": None, "fp32": ls.PREC_FP32, "bf16x3": ls.PREC_BF16X3,
+            "bf16x6": ls.PREC_BF16X6}[args.mode]
+    stream = torch.cuda.Stream(device=dev)
+    ls.set_stream(stream)
+    ls.set_sync(False)
+
+    # inputs: one buffer per (size, layout) batch, seeded, uniform [-1, 1)
+    g = torch.Generator(device=dev)
+    g.manual_seed(1234 + rank)
+    bufs = []
+    with torch.cuda.stream(stream):
+        for n in SIZES:
+            for tb in LAYOUTS:
+                A = torch.rand((BATCH, n, n), generator=g, device=dev) * 2 - 1
+                B = torch.rand((BATCH, n, n), generator=g, device=dev) * 2 - 1
+                C = torch.empty((BATCH, n, n), device=dev)
+                bufs.append((n, tb, A, B, C))
+    stream.synchronize()
+
+    def launch_all():
+        for (n, tb, A, B, C) in bufs:
+            ls.sgemm_batched_strided(tb, n, n, n, 1.0, A, n * n, B, n * n, 0.0, C, n * n, BATCH)
+
+    # pick the mode: the fastest accurate one unless forced
+    candidates = [mode] if mode is not None else [ls.PREC_FP32, ls.PREC_BF16X6]
+    results = {}
+    for m in candidates:
+        ls.set_precision(m)
+        st = ls.sgemm_batched_strided(0, 8, 8, 8, 1.0, bufs[0][2], 64, bufs[0][3], 64, 0.0,
+                                      bufs[0][4], 64, 1, check=False)
+        if st != ls.SUCCESS:
+            results[m] = {"status": ls.error_string(st)}
+            continue
+        stream.synchronize()
+        # accuracy on a sample of every batch (torch float64 on the GPU)
+        err = 0.0
+        with torch.cuda.stream(stream):
+            launch_all()
+            for (n, tb, A, B, C) in bufs:
+                a = A[:64].double()
+                b = B[:64].double()
+                ref = a @ (b.transpose(1, 2) if tb else b)
+                e = ((C[:64].double() - ref).abs().amax(dim=(1, 2)) /
+                     ref.abs().amax(dim=(1, 2))).max().item()
+                err = max(err, e)
+        stream.synchronize()
+        results[m] = {"max_normwise_err": err}
+
+    def timed(m):
+        ls.set_precision(m)
+        for _ in range(args.warmup):
+            launch_all()
+        stream.synchronize()
+        if world > 1:
+            torch.distributed.barrier()
+        torch.cuda.synchronize()
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+              for _ in range(args.steps * len(bufs))]
+        t0 = torch.cuda.Event(enable_timing=True)
+        t1 = torch.cuda.Event(enable_timing=True)
+        t0.record(stream)
+        i = 0
+        for _ in range(args.steps):
+            for (n, tb, A, B, C) in bufs:
+                ev[i][0].record(stream)
+                ls.sgemm_batched_strided(tb, n, n, n, 1.0, A, n * n, B, n * n, 0.0, C, n * n,
+                                         BATCH)
+                ev[i][1].record(stream)
+                i += 1
+        t1.record(stream)
+        stream.synchronize()
+        torch.cuda.synchronize()
+        total_ms = t0.elapsed_time(t1)
+        kern_ms = sum(a.elapsed_time(b) for a, b in ev)
+        return total_ms, kern_ms
+
+    usable = [m for m in candidates if "max_normwise_err" in results[m]]
+    for m in usable:
+        total_ms, kern_ms = timed(m)
+        results[m]["ms_per_step"] = total_ms / args.steps
+        results[m]["gflops"] = step_flops() * args.steps / (total_ms / 1e3) / 1e9
+    # headline: fastest mode meeting the FP32-class bound (1e-6), else plain
+    ok = [m for m in usable if results[m]["max_normwise_err"] <= 1e-6]
+    best = max(ok or usable, key=lambda m: results[m]["gflops"])
+
+    # final timed run of the headline mode with clocks sampled
+    clocks = Clocks(local)
+    clocks.start()
+    total_ms, kern_ms = timed(best)
+    clk = clocks.stop()
+    ms_step = total_ms / args.steps
+    if world > 1:
+        t = torch.tensor([ms_step], device=dev)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        ms_step = t.item()
+    value = world * step_flops() / (ms_step / 1e3) / 1e9
+    launches = args.steps * len(bufs)
+    kern_ms_per_launch = kern_ms / launches
+    achieved_gbs = step_bytes() / len(bufs) / (kern_ms_per_launch / 1e3) / 1e9
+
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except (OSError, ValueError):
+        pass
+    hbm_peak = float(peaks.get("hbm_gbs", 6650.0))
+    peak_src = "measured" if "hbm_gbs" in peaks else "fallback"
+
+    # e2e through the C ABI with host buffers (pinned), copies inside the timed region
+    e2e = None
+    if not args.no_e2e:
+        ls.set_precision(best)
+        host = []
+        for (n, tb, A, B, C) in bufs:
+            hA = torch.empty(A.shape, dtype=A.dtype, pin_memory=True)
+            hB = torch.empty(B.shape, dtype=B.dtype, pin_memory=True)
+            hC = torch.empty(C.shape, dtype=C.dtype, pin_memory=True)
+            hA.copy_(A.cpu())
+            hB.copy_(B.cpu())
+            host.append((hA, hB, hC))
+        h2d = sum(h[0].numel() * 4 + h[1].numel() * 4 for h in host)
+        d2h = sum(h[2].numel() * 4 for h in host)
+
+        def e2e_step():
+            for (n, tb, A, B, C), (hA, hB, hC) in zip(bufs, host):
+                A.copy_(hA, non_blocking=True)
+                B.copy_(hB, non_blocking=True)
+                ls.sgemm_batched_strided(tb, n, n, n, 1.0, A, n * n, B, n * n, 0.0, C, n * n,
+                                         BATCH)
+                hC.copy_(C, non_blocking=True)
+
+        e_steps = max(1, min(args.steps, 3))
+        with torch.cuda.stream(stream):
+            e2e_step()
+            stream.synchronize()
+            if world > 1:
+                torch.distributed.barrier()
+            s0 = torch.cuda.Event(enable_timing=True)
+            s1 = torch.cuda.Event(enable_timing=True)
+            s0.record(stream)
+            for _ in range(e_steps):
+                e2e_step()
+            s1.record(stream)
+            stream.synchronize()
+        e_ms = s0.elapsed_time(s1) / e_steps
+        if world > 1:
+            t = torch.tensor([e_ms], device=dev)
+            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+            e_ms = t.item()
+        e2e = {"value": world * step_flops() / (e_ms / 1e3) / 1e9, "unit": "GFLOP/s",
+               "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "ms_per_step": e_ms}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        v, cores, per, dt = cpu_sample()
+        model, _ = cpu_info()
+        cpu = {"value": v, "unit": "GFLOP/s", "cores": cores, "kind": "port",
+               "sample": (f"cube sweep 8..128 NN+NT with {per} GEMMs per size and layout "
+                          f"({step_flops(per) / 1e9:.1f} GFLOP in {dt:.1f} s), C restatement "
+                          f"of the reference's 5x16-tile algorithm (AArch64 NEON assembly not "
+                          f"buildable on x86), OpenMP over GEMMs on {model}")}
+
+    names = {ls.PREC_FP32: "fp32", ls.PREC_BF16X3: "bf16x3", ls.PREC_BF16X6: "bf16x6"}
+    line = {
+        "metric": METRIC, "value": value, "unit": "GFLOP/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32" if best == ls.PREC_FP32 else "f32 (bf16 split products, f32 accumulate)",
+        "data": "synthetic",
+        "config": {"workload": "cube sweep M=N=K in 8..128 step 8, NN and NT, uniform batches "
+                               "of 10,000 FP32 GEMMs per size (32 batched calls per step)",
+                   "batch_per_size": BATCH, "step_gflop": step_flops() / 1e9,
+                   "step_gbytes": step_bytes() / 1e9, "mode": names[best],
+                   "l2": "inputs larger than L2: 23 GB touched per step",
+                   "parallelism": f"replicas x{world}"},
+        "modes": {names[m]: r for m, r in results.items()},
+        "roofline": {"bound": "hbm", "achieved": achieved_gbs, "peak": hbm_peak,
+                     "unit": "GB/s", "frac": achieved_gbs / hbm_peak, "traffic": None,
+                     "peak_source": peak_src,
+                     "kernel": "sgemm batched (" + names[best] + ")",
+                     "kernel_ms_per_launch": kern_ms_per_launch},
+        "gpu_launches": launches,
+        "clocks": clk,
+        "e2e": e2e,
+        "cpu_baseline": cpu,
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        torch.distributed.barrier()
+        torch.distributed.destroy_process_group()
+    return 0
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_gpu(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

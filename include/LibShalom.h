@@ -1,0 +1,174 @@
+/*
+ * LibShalom.h -- B200 (sm_100a) small and irregular-shaped GEMM library.
+ *
+ * Drop-in C ABI for the public interface of LibShalom
+ * (NN_LIB/LibShalom.h:9-41 of the ARMv8 reference).  The five reference
+ * entry points keep their names, argument order, types and void returns;
+ * this header is plain C (the reference header needs C++ for <vector>), so
+ * callers relink against this library after recompiling.
+ *
+ * Differences a caller must know:
+ *   - A, B and C are DEVICE pointers (cudaMalloc'd or managed memory).
+ *   - Calls are synchronous by default (C is final when the call returns),
+ *     as in the reference; LibShalom_set_sync(0) makes them stream-ordered
+ *     on the stream given to LibShalom_set_stream().
+ *   - Errors: the reference silently ignores bad input (void, no checks).
+ *     Here every call records a status readable with
+ *     LibShalom_get_last_error() (per host thread); nothing is launched
+ *     for invalid arguments.
+ *   - transa: the reference ignores it (NN_LIB/NN_SMM.c:8,33 comment it
+ *     out).  Here transa == Trans means A is stored K x M (BLAS meaning).
+ *   - LibShalom_dgemm with transb == Trans: the reference does nothing
+ *     (NN_SMM.c:30-37); here it computes C = A * B^T.
+ *   - Every row and column of C is computed (the reference leaves some
+ *     tail rows/columns unwritten in DGEMM_NN and the NGM mp drivers).
+ */
+#ifndef LIBSHALOM_B200_H
+#define LIBSHALOM_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define LIBSHALOM_API __attribute__((visibility("default")))
+#else
+#define LIBSHALOM_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* NN_LIB/LibShalom.h:9-12 */
+#define NoTrans 0
+#define Trans 1
+
+/* NN_LIB/LibShalom.h:14-16: the reference's cache-blocking constants.  Here
+ * GEMM_K is the K-block at which the plain sgemm_mp path folds its running
+ * partial into C (the reference's k_tag accumulation), which keeps the
+ * plain FP32 rounding order equal to the reference mp drivers'. */
+#define GEMM_K 320
+#define GEMM_N 4096
+#define GEMM_M 256
+
+/* ---------------------------------------------------------------------- */
+/* Drop-in entry points                                                   */
+/* ---------------------------------------------------------------------- */
+
+/* C[M x N] = A[M x K] * op(B), row-major; op(B) = B (K x N) for NoTrans, B^T
+ * with B stored N x K for Trans.  Replaces NN_LIB/LibShalom.h:22
+ * (implementation NN_LIB/NN_SMM.c:5-27: SGEMM_NN / SGEMM_NN_L1 /
+ * SGEMM_NT).  Plain FP32: k-sequential fused multiply-add per element. */
+LIBSHALOM_API void LibShalom_sgemm(int transa, int transb, float *C, float *A, float *B,
+                     long M, long N, long K);
+
+/* Irregular-shaped SGEMM (tall-skinny / im2col shapes).  Replaces
+ * NN_LIB/LibShalom.h:27 (implementation NN_LIB/SMM_thread.c:75-113 and the
+ * drivers of SMM_NN_new.c / SMM_NT_new.c).  Uses the precision mode set by
+ * LibShalom_set_precision() (default plain FP32). */
+LIBSHALOM_API void LibShalom_sgemm_mp(int transa, int transb, float *C, float *A, float *B,
+                        long M, long N, long K);
+
+/* C = A * op(B) in FP64.  Replaces NN_LIB/LibShalom.h:38 (implementation
+ * NN_LIB/NN_SMM.c:30-37 -> DGEMM_NN.c:5). */
+LIBSHALOM_API void LibShalom_dgemm(int transa, int transb, double *C, double *A, double *B,
+                     long M, long N, long K);
+
+/* Replaces NN_LIB/LibShalom.h:40 (SMM_thread.c:116-130).  The reference sets
+ * its OpenMP thread count; here num caps the number of CTAs resident at once
+ * for every kernel of the library (num <= 0 removes the cap: all SMs). */
+LIBSHALOM_API void LibShalom_set_thread_nums(int num);
+
+/* Replaces NN_LIB/LibShalom.h:41 (SMM_thread.c:132-137).  Forces the
+ * tm x tn partition of C for the NEXT LibShalom_sgemm_mp call only (the
+ * reference resets Tm after each mp call, SMM_thread.c:112): the C tile grid
+ * is split into tm x tn rectangular groups, one CTA per group. */
+LIBSHALOM_API void LibShalom_set_thread_ways(int tm, int tn);
+
+/* ---------------------------------------------------------------------- */
+/* Status and execution control (no counterpart in the reference, which   */
+/* has no error reporting)                                                 */
+/* ---------------------------------------------------------------------- */
+
+#define LIBSHALOM_SUCCESS 0
+#define LIBSHALOM_ERR_INVALID_VALUE 1 /* bad size, pointer, trans or mode */
+#define LIBSHALOM_ERR_UNSUPPORTED 2   /* valid request this build cannot run */
+#define LIBSHALOM_ERR_CUDA 3          /* a CUDA runtime call failed */
+#define LIBSHALOM_ERR_NO_DEVICE 4     /* no sm_100 device visible */
+#define LIBSHALOM_ERR_ALLOC 5         /* workspace allocation failed */
+#define LIBSHALOM_ERR_DEVICE_TIMEOUT 6 /* a bounded device-side wait expired */
+
+/* Status of the last library call made by this host thread. */
+LIBSHALOM_API int LibShalom_get_last_error(void);
+/* Static description of a status code. */
+LIBSHALOM_API const char *LibShalom_error_string(int status);
+
+/* Stream for all later launches (a cudaStream_t; NULL = default stream). */
+LIBSHALOM_API int LibShalom_set_stream(void *stream);
+/* 1 (default): calls return after the result is written.  0: calls are
+ * stream-ordered and return after the launch. */
+LIBSHALOM_API int LibShalom_set_sync(int synchronous);
+/* Wait for all work the library queued on its stream. */
+LIBSHALOM_API int LibShalom_synchronize(void);
+
+/* Arithmetic of LibShalom_sgemm_mp and LibShalom_sgemm_batched*. */
+#define LIBSHALOM_PREC_FP32 0   /* plain FP32 FMA on the CUDA cores */
+#define LIBSHALOM_PREC_BF16X3 1 /* hi/lo BF16 split, 3 tcgen05 products */
+#define LIBSHALOM_PREC_BF16X6 2 /* hi/mid/lo BF16 split, 6 tcgen05 products */
+LIBSHALOM_API int LibShalom_set_precision(int mode);
+LIBSHALOM_API int LibShalom_get_precision(void);
+
+/* Split-K factor for LibShalom_sgemm_mp: 0 = chosen by the tile scheduler
+ * (default), 1 = never split, s > 1 = split K into s slices. */
+LIBSHALOM_API int LibShalom_set_splitk(int splits);
+
+/* Release the library's device workspace and cached plans. */
+LIBSHALOM_API void LibShalom_finalize(void);
+
+/* ---------------------------------------------------------------------- */
+/* Batched entry points (no counterpart in the reference)                 */
+/* ---------------------------------------------------------------------- */
+
+/* One GEMM of a grouped batch: C = alpha * A * op(B) + beta * C, row-major.
+ * lda/ldb/ldc <= 0 select the packed defaults (K, N or K, N). */
+typedef struct LibShalom_sgemm_entry {
+  const float *A;
+  const float *B;
+  float *C;
+  int32_t M, N, K;
+  int32_t transb;
+  int32_t lda, ldb, ldc;
+  float alpha, beta;
+  int32_t reserved;
+} LibShalom_sgemm_entry; /* 64 bytes */
+
+typedef struct LibShalom_dgemm_entry {
+  const double *A;
+  const double *B;
+  double *C;
+  int32_t M, N, K;
+  int32_t transb;
+  int32_t lda, ldb, ldc;
+  int32_t reserved;
+  double alpha, beta;
+} LibShalom_dgemm_entry; /* 72 bytes */
+
+/* Grouped SGEMM over `count` entries that live in DEVICE memory.  Entries
+ * are independent unless they name the same C; entries that share a C must
+ * be contiguous in the array and are applied in array order by one CTA. */
+LIBSHALOM_API int LibShalom_sgemm_batched(const LibShalom_sgemm_entry *entries, long count);
+
+/* Uniform batch: count GEMMs of one shape, matrix g at A + g*strideA etc. */
+LIBSHALOM_API int LibShalom_sgemm_batched_strided(int transb, long M, long N, long K,
+                                    float alpha, const float *A, long strideA,
+                                    const float *B, long strideB, float beta,
+                                    float *C, long strideC, long count);
+
+/* Grouped DGEMM (same rules as LibShalom_sgemm_batched; FP64 FMA). */
+LIBSHALOM_API int LibShalom_dgemm_batched(const LibShalom_dgemm_entry *entries, long count);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* LIBSHALOM_B200_H */

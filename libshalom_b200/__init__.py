@@ -1,0 +1,262 @@
+"""Python host binding of the B200 LibShalom C ABI (``include/LibShalom.h``).
+
+Every function here forwards to ``libshalom_b200.so`` through ctypes with
+plain device pointers and sizes; there is no fallback: if the shared library
+is missing or cannot be loaded, importing the compute entry points raises.
+Torch tensors are accepted for convenience (their ``data_ptr()`` is passed);
+torch is plumbing here (device memory, streams), not the compute path.
+
+The reference interface mirrored here is ``NN_LIB/LibShalom.h:9-41``
+(``LibShalom_sgemm``, ``LibShalom_sgemm_mp``, ``LibShalom_dgemm``,
+``LibShalom_set_thread_nums``, ``LibShalom_set_thread_ways``).
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libshalom_b200.so")
+INCLUDE_DIR = os.path.join(os.path.dirname(_HERE), "include")
+
+NoTrans = 0
+Trans = 1
+GEMM_K = 320
+GEMM_N = 4096
+GEMM_M = 256
+
+SUCCESS = 0
+ERR_INVALID_VALUE = 1
+ERR_UNSUPPORTED = 2
+ERR_CUDA = 3
+ERR_NO_DEVICE = 4
+ERR_ALLOC = 5
+ERR_DEVICE_TIMEOUT = 6
+
+PREC_FP32 = 0
+PREC_BF16X3 = 1
+PREC_BF16X6 = 2
+
+# every symbol include/LibShalom.h declares
+EXPORTED = (
+    "LibShalom_sgemm", "LibShalom_sgemm_mp", "LibShalom_dgemm",
+    "LibShalom_set_thread_nums", "LibShalom_set_thread_ways",
+    "LibShalom_get_last_error", "LibShalom_error_string",
+    "LibShalom_set_stream", "LibShalom_set_sync", "LibShalom_synchronize",
+    "LibShalom_set_precision", "LibShalom_get_precision", "LibShalom_set_splitk",
+    "LibShalom_finalize",
+    "LibShalom_sgemm_batched", "LibShalom_sgemm_batched_strided",
+    "LibShalom_dgemm_batched",
+)
+
+_L = ctypes.c_long
+_I = ctypes.c_int
+_P = ctypes.c_void_p
+_F = ctypes.c_float
+
+
+class SgemmEntry(ctypes.Structure):
+    """LibShalom_sgemm_entry (64 bytes)."""
+    _fields_ = [("A", _P), ("B", _P), ("C", _P),
+                ("M", ctypes.c_int32), ("N", ctypes.c_int32), ("K", ctypes.c_int32),
+                ("transb", ctypes.c_int32),
+                ("lda", ctypes.c_int32), ("ldb", ctypes.c_int32), ("ldc", ctypes.c_int32),
+                ("alpha", ctypes.c_float), ("beta", ctypes.c_float),
+                ("reserved", ctypes.c_int32)]
+
+
+class DgemmEntry(ctypes.Structure):
+    """LibShalom_dgemm_entry (72 bytes)."""
+    _fields_ = [("A", _P), ("B", _P), ("C", _P),
+                ("M", ctypes.c_int32), ("N", ctypes.c_int32), ("K", ctypes.c_int32),
+                ("transb", ctypes.c_int32),
+                ("lda", ctypes.c_int32), ("ldb", ctypes.c_int32), ("ldc", ctypes.c_int32),
+                ("reserved", ctypes.c_int32),
+                ("alpha", ctypes.c_double), ("beta", ctypes.c_double)]
+
+
+assert ctypes.sizeof(SgemmEntry) == 64 and ctypes.sizeof(DgemmEntry) == 72
+
+_SIGS = {
+    "LibShalom_sgemm": (None, [_I, _I, _P, _P, _P, _L, _L, _L]),
+    "LibShalom_sgemm_mp": (None, [_I, _I, _P, _P, _P, _L, _L, _L]),
+    "LibShalom_dgemm": (None, [_I, _I, _P, _P, _P, _L, _L, _L]),
+    "LibShalom_set_thread_nums": (None, [_I]),
+    "LibShalom_set_thread_ways": (None, [_I, _I]),
+    "LibShalom_get_last_error": (_I, []),
+    "LibShalom_error_string": (ctypes.c_char_p, [_I]),
+    "LibShalom_set_stream": (_I, [_P]),
+    "LibShalom_set_sync": (_I, [_I]),
+    "LibShalom_synchronize": (_I, []),
+    "LibShalom_set_precision": (_I, [_I]),
+    "LibShalom_get_precision": (_I, []),
+    "LibShalom_set_splitk": (_I, [_I]),
+    "LibShalom_finalize": (None, []),
+    "LibShalom_sgemm_batched": (_I, [_P, _L]),
+    "LibShalom_sgemm_batched_strided": (_I, [_I, _L, _L, _L, _F, _P, _L, _P, _L, _F, _P, _L,
+                                             _L]),
+    "LibShalom_dgemm_batched": (_I, [_P, _L]),
+}
+
+_lib = None
+
+
+class LibShalomError(RuntimeError):
+    def __init__(self, status: int, what: str = ""):
+        self.status = status
+        super().__init__(f"{what}: {error_string(status)} (status {status})")
+
+
+def lib() -> ctypes.CDLL:
+    """The loaded C library.  Raises if it is missing (no CPU fallback)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(f"{LIB_PATH} is missing: run __graft_entry__.build() "
+                              "(make -C libshalom_b200/csrc)")
+        L = ctypes.CDLL(LIB_PATH)
+        for name, (res, args) in _SIGS.items():
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = L
+    return _lib
+
+
+def error_string(status: int) -> str:
+    return lib().LibShalom_error_string(int(status)).decode()
+
+
+def last_error() -> int:
+    return lib().LibShalom_get_last_error()
+
+
+def _ptr(x) -> int | None:
+    if x is None:
+        return None
+    if isinstance(x, int):
+        return x
+    return x.data_ptr()
+
+
+def _check(status: int, what: str) -> None:
+    if status != SUCCESS:
+        raise LibShalomError(status, what)
+
+
+# --------------------------------------------------------------------------
+# drop-in entry points (void in C: status read back with get_last_error)
+# --------------------------------------------------------------------------
+
+def sgemm(transa, transb, C, A, B, M, N, K, check=True) -> int:
+    lib().LibShalom_sgemm(transa, transb, _ptr(C), _ptr(A), _ptr(B), M, N, K)
+    st = last_error()
+    if check:
+        _check(st, "LibShalom_sgemm")
+    return st
+
+
+def sgemm_mp(transa, transb, C, A, B, M, N, K, check=True) -> int:
+    lib().LibShalom_sgemm_mp(transa, transb, _ptr(C), _ptr(A), _ptr(B), M, N, K)
+    st = last_error()
+    if check:
+        _check(st, "LibShalom_sgemm_mp")
+    return st
+
+
+def dgemm(transa, transb, C, A, B, M, N, K, check=True) -> int:
+    lib().LibShalom_dgemm(transa, transb, _ptr(C), _ptr(A), _ptr(B), M, N, K)
+    st = last_error()
+    if check:
+        _check(st, "LibShalom_dgemm")
+    return st
+
+
+def set_thread_nums(num: int) -> None:
+    lib().LibShalom_set_thread_nums(int(num))
+
+
+def set_thread_ways(tm: int, tn: int) -> None:
+    lib().LibShalom_set_thread_ways(int(tm), int(tn))
+    _check(last_error(), "LibShalom_set_thread_ways")
+
+
+# --------------------------------------------------------------------------
+# execution control
+# --------------------------------------------------------------------------
+
+def set_stream(stream) -> None:
+    """stream: a torch.cuda.Stream, a raw cudaStream_t int, or None."""
+    handle = None if stream is None else (stream if isinstance(stream, int)
+                                          else stream.cuda_stream)
+    _check(lib().LibShalom_set_stream(handle), "LibShalom_set_stream")
+
+
+def set_sync(on: bool) -> None:
+    _check(lib().LibShalom_set_sync(1 if on else 0), "LibShalom_set_sync")
+
+
+def synchronize() -> None:
+    _check(lib().LibShalom_synchronize(), "LibShalom_synchronize")
+
+
+def set_precision(mode: int) -> None:
+    _check(lib().LibShalom_set_precision(int(mode)), "LibShalom_set_precision")
+
+
+def get_precision() -> int:
+    return lib().LibShalom_get_precision()
+
+
+def set_splitk(splits: int) -> None:
+    _check(lib().LibShalom_set_splitk(int(splits)), "LibShalom_set_splitk")
+
+
+def finalize() -> None:
+    lib().LibShalom_finalize()
+
+
+# --------------------------------------------------------------------------
+# batched entry points
+# --------------------------------------------------------------------------
+
+def sgemm_batched(entries_dev, count: int, check=True) -> int:
+    """entries_dev: device buffer (tensor or pointer) of `count` SgemmEntry."""
+    st = lib().LibShalom_sgemm_batched(_ptr(entries_dev), int(count))
+    if check:
+        _check(st, "LibShalom_sgemm_batched")
+    return st
+
+
+def sgemm_batched_strided(transb, M, N, K, alpha, A, strideA, B, strideB, beta, C, strideC,
+                          count, check=True) -> int:
+    st = lib().LibShalom_sgemm_batched_strided(transb, M, N, K, alpha, _ptr(A), strideA,
+                                               _ptr(B), strideB, beta, _ptr(C), strideC, count)
+    if check:
+        _check(st, "LibShalom_sgemm_batched_strided")
+    return st
+
+
+def dgemm_batched(entries_dev, count: int, check=True) -> int:
+    st = lib().LibShalom_dgemm_batched(_ptr(entries_dev), int(count))
+    if check:
+        _check(st, "LibShalom_dgemm_batched")
+    return st
+
+
+def pack_entries(entries) -> bytes:
+    """Serialise a list of SgemmEntry/DgemmEntry structures to bytes."""
+    return b"".join(bytes(e) for e in entries)
+
+
+# numpy views of the entry structures (for building large batches quickly)
+def entry_dtypes():
+    import numpy as np
+    s = np.dtype([("A", "<u8"), ("B", "<u8"), ("C", "<u8"), ("M", "<i4"), ("N", "<i4"),
+                  ("K", "<i4"), ("transb", "<i4"), ("lda", "<i4"), ("ldb", "<i4"),
+                  ("ldc", "<i4"), ("alpha", "<f4"), ("beta", "<f4"), ("reserved", "<i4")])
+    d = np.dtype([("A", "<u8"), ("B", "<u8"), ("C", "<u8"), ("M", "<i4"), ("N", "<i4"),
+                  ("K", "<i4"), ("transb", "<i4"), ("lda", "<i4"), ("ldb", "<i4"),
+                  ("ldc", "<i4"), ("reserved", "<i4"), ("alpha", "<f8"), ("beta", "<f8")])
+    assert s.itemsize == 64 and d.itemsize == 72
+    return s, d

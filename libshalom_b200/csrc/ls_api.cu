@@ -1,0 +1,342 @@
+// ls_api.cu -- the C ABI of include/LibShalom.h: argument checking, library
+// state, workspace and dispatch to the kernels.
+#include <cuda_runtime.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include <algorithm>
+#include <unordered_map>
+
+#include "ls_common.cuh"
+#include "ls_simt_launch.h"
+#include "ls_tc_launch.h"
+
+namespace ls {
+
+static thread_local int t_last_error = LIBSHALOM_SUCCESS;
+
+void set_error(int status) { t_last_error = status; }
+int last_error() { return t_last_error; }
+
+void note_cuda_error(cudaError_t e, const char *what, const char *file, int line) {
+  if (getenv("LIBSHALOM_DEBUG"))
+    fprintf(stderr, "libshalom: %s failed: %s (%s:%d)\n", what, cudaGetErrorString(e), file,
+            line);
+}
+
+State &state() {
+  static State s;
+  return s;
+}
+
+int ensure_device() {
+  State &st = state();
+  int dev = -1;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) {
+    note_cuda_error(e, "cudaGetDevice", __FILE__, __LINE__);
+    return LIBSHALOM_ERR_NO_DEVICE;
+  }
+  if (dev == st.device) return LIBSHALOM_SUCCESS;
+  cudaDeviceProp prop;
+  e = cudaGetDeviceProperties(&prop, dev);
+  if (e != cudaSuccess) {
+    note_cuda_error(e, "cudaGetDeviceProperties", __FILE__, __LINE__);
+    return LIBSHALOM_ERR_NO_DEVICE;
+  }
+  if (prop.major != 10) return LIBSHALOM_ERR_NO_DEVICE;  // built for sm_100a only
+  st.device = dev;
+  st.num_sms = prop.multiProcessorCount;
+  st.cc_major = prop.major;
+  st.cc_minor = prop.minor;
+  st.smem_optin = prop.sharedMemPerBlockOptin;
+  return LIBSHALOM_SUCCESS;
+}
+
+int workspace(size_t bytes, void **out) {
+  State &st = state();
+  if (bytes < 256) bytes = 256;
+  if (st.ws && st.ws_bytes >= bytes && st.ws_device == st.device) {
+    *out = st.ws;
+    return LIBSHALOM_SUCCESS;
+  }
+  if (st.ws) {
+    // kernels queued earlier may still read the old buffer
+    LS_CUDA_TRY(cudaStreamSynchronize(st.stream));
+    cudaFree(st.ws);
+    st.ws = nullptr;
+    st.ws_bytes = 0;
+  }
+  size_t want = std::max(bytes, (size_t)1 << 20);
+  if (cudaMalloc(&st.ws, want) != cudaSuccess) {
+    cudaGetLastError();
+    st.ws = nullptr;
+    return LIBSHALOM_ERR_ALLOC;
+  }
+  st.ws_bytes = want;
+  st.ws_device = st.device;
+  *out = st.ws;
+  return LIBSHALOM_SUCCESS;
+}
+
+int grid_for(long work_items, int per_sm) {
+  State &st = state();
+  long slots = (long)st.num_sms * std::max(per_sm, 1);
+  if (st.thread_cap > 0) slots = std::min<long>(slots, st.thread_cap);
+  long g = std::min(work_items, slots);
+  return (int)std::max(g, 1L);
+}
+
+int occupancy_of(const void *kern, int threads, size_t smem, int fallback) {
+  static std::mutex m;
+  static std::unordered_map<const void *, int> cache;
+  std::lock_guard<std::mutex> lk(m);
+  auto it = cache.find(kern);
+  if (it != cache.end()) return it->second;
+  if (smem > 48 * 1024 &&
+      cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
+          cudaSuccess) {
+    cudaGetLastError();
+    return fallback;
+  }
+  int n = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kern, threads, smem) != cudaSuccess ||
+      n <= 0) {
+    cudaGetLastError();
+    return fallback;
+  }
+  cache[kern] = n;
+  return n;
+}
+
+int finish_launch(const char *what) {
+  State &st = state();
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) {
+    note_cuda_error(e, what, __FILE__, __LINE__);
+    return LIBSHALOM_ERR_CUDA;
+  }
+  if (st.sync) {
+    e = cudaStreamSynchronize(st.stream);
+    if (e != cudaSuccess) {
+      note_cuda_error(e, what, __FILE__, __LINE__);
+      return LIBSHALOM_ERR_CUDA;
+    }
+  }
+  return LIBSHALOM_SUCCESS;
+}
+
+template <typename T>
+static int gemm_common(int transa, int transb, T *C, const T *A, const T *B, long M, long N,
+                       long K, bool mp) {
+  if ((transa != NoTrans && transa != Trans) || (transb != NoTrans && transb != Trans))
+    return LIBSHALOM_ERR_INVALID_VALUE;
+  if (M < 0 || N < 0 || K < 0) return LIBSHALOM_ERR_INVALID_VALUE;
+  if (M == 0 || N == 0) return LIBSHALOM_SUCCESS;
+  if (!C || (K > 0 && (!A || !B))) return LIBSHALOM_ERR_INVALID_VALUE;
+  // int32 tile indices inside the kernels
+  if (M > (1L << 30) || N > (1L << 30) || K > (1L << 40)) return LIBSHALOM_ERR_INVALID_VALUE;
+  int rc = ensure_device();
+  if (rc) return rc;
+  State &st = state();
+  GemmArgs<T> g;
+  g.A = A; g.B = B; g.C = C;
+  g.M = M; g.N = N; g.K = K;
+  g.transa = transa; g.transb = transb;
+  g.lda = transa ? M : K;
+  g.ldb = transb ? K : N;
+  g.ldc = N;
+  g.alpha = T(1); g.beta = T(0);
+  SimtOptions opt;
+  if (mp) {
+    opt.kblock = true;
+    opt.splits = st.splitk;
+    opt.allow_split = st.splitk != 1;
+    opt.ways_m = st.ways_m;
+    opt.ways_n = st.ways_n;
+    st.ways_m = st.ways_n = 0;  // one-shot, like the reference's Tm = 0 reset
+  } else {
+    opt.allow_split = false;
+  }
+  if (mp && sizeof(T) == 4 && st.precision != LIBSHALOM_PREC_FP32) {
+    rc = tc_sgemm_single((const GemmArgs<float> &)g, st.precision, opt.splits);
+  } else {
+    rc = run_gemm<T>(g, opt, nullptr);
+  }
+  if (rc) return rc;
+  return finish_launch("gemm");
+}
+
+}  // namespace ls
+
+using namespace ls;
+
+extern "C" {
+
+void LibShalom_sgemm(int transa, int transb, float *C, float *A, float *B, long M, long N,
+                     long K) {
+  std::lock_guard<std::mutex> lk(state().mu);
+  set_error(gemm_common<float>(transa, transb, C, A, B, M, N, K, false));
+}
+
+void LibShalom_sgemm_mp(int transa, int transb, float *C, float *A, float *B, long M, long N,
+                        long K) {
+  std::lock_guard<std::mutex> lk(state().mu);
+  set_error(gemm_common<float>(transa, transb, C, A, B, M, N, K, true));
+}
+
+void LibShalom_dgemm(int transa, int transb, double *C, double *A, double *B, long M, long N,
+                     long K) {
+  std::lock_guard<std::mutex> lk(state().mu);
+  set_error(gemm_common<double>(transa, transb, C, A, B, M, N, K, false));
+}
+
+void LibShalom_set_thread_nums(int num) {
+  std::lock_guard<std::mutex> lk(state().mu);
+  state().thread_cap = num > 0 ? num : 0;
+  set_error(LIBSHALOM_SUCCESS);
+}
+
+void LibShalom_set_thread_ways(int tm, int tn) {
+  std::lock_guard<std::mutex> lk(state().mu);
+  if (tm <= 0 || tn <= 0) {
+    set_error(LIBSHALOM_ERR_INVALID_VALUE);
+    return;
+  }
+  state().ways_m = tm;
+  state().ways_n = tn;
+  set_error(LIBSHALOM_SUCCESS);
+}
+
+int LibShalom_get_last_error(void) { return last_error(); }
+
+const char *LibShalom_error_string(int status) {
+  switch (status) {
+    case LIBSHALOM_SUCCESS: return "success";
+    case LIBSHALOM_ERR_INVALID_VALUE: return "invalid argument";
+    case LIBSHALOM_ERR_UNSUPPORTED: return "unsupported request";
+    case LIBSHALOM_ERR_CUDA: return "CUDA runtime error";
+    case LIBSHALOM_ERR_NO_DEVICE: return "no sm_100 device";
+    case LIBSHALOM_ERR_ALLOC: return "device workspace allocation failed";
+    case LIBSHALOM_ERR_DEVICE_TIMEOUT: return "bounded device wait expired";
+  }
+  return "unknown status";
+}
+
+int LibShalom_set_stream(void *stream) {
+  std::lock_guard<std::mutex> lk(state().mu);
+  state().stream = reinterpret_cast<cudaStream_t>(stream);
+  set_error(LIBSHALOM_SUCCESS);
+  return LIBSHALOM_SUCCESS;
+}
+
+int LibShalom_set_sync(int synchronous) {
+  std::lock_guard<std::mutex> lk(state().mu);
+  state().sync = synchronous ? 1 : 0;
+  set_error(LIBSHALOM_SUCCESS);
+  return LIBSHALOM_SUCCESS;
+}
+
+int LibShalom_synchronize(void) {
+  std::lock_guard<std::mutex> lk(state().mu);
+  cudaError_t e = cudaStreamSynchronize(state().stream);
+  int rc = e == cudaSuccess ? LIBSHALOM_SUCCESS : LIBSHALOM_ERR_CUDA;
+  if (rc) note_cuda_error(e, "cudaStreamSynchronize", __FILE__, __LINE__);
+  set_error(rc);
+  return rc;
+}
+
+int LibShalom_set_precision(int mode) {
+  std::lock_guard<std::mutex> lk(state().mu);
+  int rc = LIBSHALOM_SUCCESS;
+  if (mode != LIBSHALOM_PREC_FP32 && mode != LIBSHALOM_PREC_BF16X3 &&
+      mode != LIBSHALOM_PREC_BF16X6)
+    rc = LIBSHALOM_ERR_INVALID_VALUE;
+  else
+    state().precision = mode;
+  set_error(rc);
+  return rc;
+}
+
+int LibShalom_get_precision(void) { return state().precision; }
+
+int LibShalom_set_splitk(int splits) {
+  std::lock_guard<std::mutex> lk(state().mu);
+  int rc = LIBSHALOM_SUCCESS;
+  if (splits < 0) rc = LIBSHALOM_ERR_INVALID_VALUE;
+  else state().splitk = splits;
+  set_error(rc);
+  return rc;
+}
+
+void LibShalom_finalize(void) {
+  std::lock_guard<std::mutex> lk(state().mu);
+  State &st = state();
+  if (st.ws) {
+    cudaStreamSynchronize(st.stream);
+    cudaFree(st.ws);
+  }
+  st.ws = nullptr;
+  st.ws_bytes = 0;
+  st.ws_device = -1;
+  set_error(LIBSHALOM_SUCCESS);
+}
+
+static bool entries_ok(const void *entries, long count) {
+  return count >= 0 && (count == 0 || entries != nullptr);
+}
+
+int LibShalom_sgemm_batched(const LibShalom_sgemm_entry *entries, long count) {
+  std::lock_guard<std::mutex> lk(state().mu);
+  int rc = LIBSHALOM_SUCCESS;
+  if (!entries_ok(entries, count)) rc = LIBSHALOM_ERR_INVALID_VALUE;
+  else if (count > 0 && !(rc = ensure_device())) {
+    if (state().precision == LIBSHALOM_PREC_FP32) rc = run_grouped_s(entries, count);
+    else rc = tc_sgemm_grouped(entries, count, state().precision);
+    if (!rc) rc = finish_launch("sgemm_batched");
+  }
+  set_error(rc);
+  return rc;
+}
+
+int LibShalom_sgemm_batched_strided(int transb, long M, long N, long K, float alpha,
+                                    const float *A, long strideA, const float *B, long strideB,
+                                    float beta, float *C, long strideC, long count) {
+  std::lock_guard<std::mutex> lk(state().mu);
+  int rc = LIBSHALOM_SUCCESS;
+  if ((transb != NoTrans && transb != Trans) || M < 0 || N < 0 || K < 0 || count < 0 ||
+      strideA < 0 || strideB < 0 || strideC < 0)
+    rc = LIBSHALOM_ERR_INVALID_VALUE;
+  else if (count > 0 && M > 0 && N > 0 && (!C || (K > 0 && (!A || !B))))
+    rc = LIBSHALOM_ERR_INVALID_VALUE;
+  else if (count > 0 && M > 0 && N > 0 && !(rc = ensure_device())) {
+    GemmArgs<float> g;
+    g.A = A; g.B = B; g.C = C;
+    g.M = M; g.N = N; g.K = K;
+    g.transa = 0; g.transb = transb;
+    g.lda = K; g.ldb = transb ? K : N; g.ldc = N;
+    g.alpha = alpha; g.beta = beta;
+    if (state().precision == LIBSHALOM_PREC_FP32)
+      rc = run_strided<float>(g, strideA, strideB, strideC, count);
+    else
+      rc = tc_sgemm_strided(g, strideA, strideB, strideC, count, state().precision);
+    if (!rc) rc = finish_launch("sgemm_batched_strided");
+  }
+  set_error(rc);
+  return rc;
+}
+
+int LibShalom_dgemm_batched(const LibShalom_dgemm_entry *entries, long count) {
+  std::lock_guard<std::mutex> lk(state().mu);
+  int rc = LIBSHALOM_SUCCESS;
+  if (!entries_ok(entries, count)) rc = LIBSHALOM_ERR_INVALID_VALUE;
+  else if (count > 0 && !(rc = ensure_device())) {
+    rc = run_grouped_d(entries, count);
+    if (!rc) rc = finish_launch("dgemm_batched");
+  }
+  set_error(rc);
+  return rc;
+}
+
+}  // extern "C"

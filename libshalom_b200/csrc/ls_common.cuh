@@ -1,0 +1,79 @@
+// ls_common.cuh -- shared state, status codes and launch helpers of the
+// B200 LibShalom library.  Host code only sees plain pointers and sizes;
+// nothing here depends on torch.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <mutex>
+
+#include "../../include/LibShalom.h"
+
+namespace ls {
+
+// ---------------------------------------------------------------------------
+// status
+// ---------------------------------------------------------------------------
+void set_error(int status);  // records the status for this host thread
+int last_error();
+
+#define LS_CUDA_TRY(expr)                                   \
+  do {                                                      \
+    cudaError_t _e = (expr);                                \
+    if (_e != cudaSuccess) {                                \
+      ::ls::note_cuda_error(_e, #expr, __FILE__, __LINE__); \
+      return LIBSHALOM_ERR_CUDA;                            \
+    }                                                       \
+  } while (0)
+
+void note_cuda_error(cudaError_t e, const char *what, const char *file,
+                     int line);
+
+// ---------------------------------------------------------------------------
+// library state (one instance per process; guarded by mu)
+// ---------------------------------------------------------------------------
+struct State {
+  std::mutex mu;
+  int device = -1;
+  int num_sms = 0;
+  int cc_major = 0, cc_minor = 0;
+  size_t smem_optin = 0;
+  cudaStream_t stream = nullptr;
+  int sync = 1;
+  int thread_cap = 0;        // LibShalom_set_thread_nums; <=0 = no cap
+  int ways_m = 0, ways_n = 0;  // LibShalom_set_thread_ways (one-shot)
+  int precision = LIBSHALOM_PREC_FP32;
+  int splitk = 0;
+  // device workspace (split-K partials, work counters, work lists)
+  void *ws = nullptr;
+  size_t ws_bytes = 0;
+  int ws_device = -1;
+};
+
+State &state();
+
+// Makes sure a device is current and its properties are cached.  Returns a
+// LIBSHALOM_* status.
+int ensure_device();
+
+// Device workspace of at least `bytes` bytes (grown on demand, stream
+// ordered: the caller's stream is synchronised before a regrow).
+int workspace(size_t bytes, void **out);
+
+// Number of CTAs to launch for `work_items` independent items of a kernel
+// with `per_sm` resident CTAs per SM, honouring LibShalom_set_thread_nums.
+int grid_for(long work_items, int per_sm);
+
+// Resident CTAs per SM of `kern` at `threads` threads and `smem` dynamic
+// shared bytes (raises the kernel's dynamic shared-memory limit when needed;
+// cached per kernel).  Returns `fallback` if the query fails.
+int occupancy_of(const void *kern, int threads, size_t smem, int fallback);
+
+// After a launch: check the launch, and synchronise when the library runs in
+// synchronous mode.  Returns a LIBSHALOM_* status.
+int finish_launch(const char *what);
+
+inline long cdiv(long a, long b) { return (a + b - 1) / b; }
+
+}  // namespace ls

@@ -1,0 +1,31 @@
+// ls_simt_launch.h -- host-side entry points of the plain CUDA-core kernels.
+#pragma once
+
+#include "../../include/LibShalom.h"
+#include "ls_simt.cuh"
+
+namespace ls {
+
+struct SimtOptions {
+  bool allow_split = true;  // let the scheduler split K across CTAs
+  int splits = 0;           // >0 forces the split factor
+  bool kblock = false;      // GEMM_K = 320 fold (reference mp rounding order)
+  int ways_m = 0, ways_n = 0;  // LibShalom_set_thread_ways partition
+  int force_cfg = -1;       // tile configuration override (autotuner/tests)
+};
+
+struct SimtPlan {
+  int cfg = -1, bm = 0, bn = 0, splits = 1;
+  long kchunk = 0;
+};
+
+template <typename T>
+int run_gemm(const GemmArgs<T> &g, const SimtOptions &opt, SimtPlan *plan_out);
+
+template <typename T>
+int run_strided(const GemmArgs<T> &g, long sA, long sB, long sC, long count);
+
+int run_grouped_s(const LibShalom_sgemm_entry *entries, long count);
+int run_grouped_d(const LibShalom_dgemm_entry *entries, long count);
+
+}  // namespace ls

@@ -1,0 +1,19 @@
+// ls_tc_launch.h -- host-side entry points of the split-BF16 tcgen05 kernels.
+#pragma once
+
+#include "../../include/LibShalom.h"
+#include "ls_simt.cuh"
+
+namespace ls {
+
+// Single (irregular) SGEMM on the tensor cores; `mode` is a
+// LIBSHALOM_PREC_BF16X* value, `splits` as LibShalom_set_splitk.
+int tc_sgemm_single(const GemmArgs<float> &g, int mode, int splits);
+
+// Uniform batch on the tensor cores.
+int tc_sgemm_strided(const GemmArgs<float> &g, long sA, long sB, long sC, long count, int mode);
+
+// Grouped batch (entries in device memory) on the tensor cores.
+int tc_sgemm_grouped(const LibShalom_sgemm_entry *entries, long count, int mode);
+
+}  // namespace ls

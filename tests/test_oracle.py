@@ -1,0 +1,133 @@
+"""CPU checks of the oracle (the checker itself): generators against glibc,
+restatements against each other and against the exact-math oracle, and the
+committed golden fixtures."""
+import ctypes
+import glob
+import os
+
+import numpy as np
+import pytest
+
+from oracle import oracle as orc
+from tests._util import componentwise_err, fp32_bound, normwise_err
+
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
+
+
+def _glibc():
+    libc = ctypes.CDLL("libc.so.6")
+    libc.srand48.argtypes = [ctypes.c_long]
+    libc.drand48.restype = ctypes.c_double
+    return libc
+
+
+@pytest.mark.parametrize("seed", [0, 1, 17, 123456789])
+def test_drand48_matches_glibc(seed):
+    libc = _glibc()
+    libc.srand48(seed)
+    want = np.array([libc.drand48() for _ in range(1000)])
+    got = orc.drand48(seed, 1000)
+    assert np.array_equal(got, want)
+    # jump-ahead agrees with sequential draws
+    assert np.array_equal(orc.drand48(seed, 10, skip=990), want[990:])
+
+
+def test_uniform_matches_reference_random_matrix():
+    # random_matrix(): a[i*n+j] = 2.0 * (float)drand48() - 1.0 stored to float
+    # (benchmark/small_SGEMM/LibShalom_sgemm.c:26-34)
+    libc = _glibc()
+    libc.srand48(0)
+    want = np.empty(500, np.float32)
+    for i in range(500):
+        f = np.float32(libc.drand48())
+        want[i] = np.float32(2.0 * np.float64(f) - 1.0)
+    got = orc.uniform_f32(0, 500)
+    assert np.array_equal(got, want)
+    assert got.min() >= -1.0 and got.max() < 1.0
+
+
+@pytest.mark.parametrize("transb", [0, 1])
+@pytest.mark.parametrize("M,N,K", [(1, 1, 1), (5, 16, 8), (7, 9, 13), (80, 80, 80),
+                                   (33, 17, 65)])
+def test_kseq_within_fp32_bound(M, N, K, transb):
+    A, B = orc.gemm_inputs_f32(3, M, N, K, transb)
+    ref = orc.sgemm_f64(A, B, transb)
+    C = orc.sgemm_kseq(A, B, transb)
+    ab = orc.sgemm_absprod(A, B, transb)
+    assert componentwise_err(C, ref, ab) <= fp32_bound(K)
+
+
+@pytest.mark.parametrize("transb", [0, 1])
+@pytest.mark.parametrize("M,N,K", [(1, 1, 1), (5, 16, 8), (7, 9, 13), (80, 80, 80),
+                                   (6, 37, 3), (130, 70, 33)])
+def test_port_equals_kseq(M, N, K, transb):
+    # the 5x16-tile CPU port keeps the k-sequential FMA order of the reference
+    A, B = orc.gemm_inputs_f32(5, M, N, K, transb)
+    assert np.array_equal(orc.port_sgemm(A, B, transb), orc.sgemm_kseq(A, B, transb))
+
+
+@pytest.mark.parametrize("threads", [1, 4, 8])
+@pytest.mark.parametrize("transb", [0, 1])
+@pytest.mark.parametrize("M,N,K", [(64, 300, 700), (300, 20, 641), (33, 65, 320)])
+def test_port_mp_equals_kblocked(M, N, K, transb, threads):
+    A, B = orc.gemm_inputs_f32(9, M, N, K, transb)
+    got = orc.port_sgemm_mp(A, B, transb, threads)
+    assert np.array_equal(got, orc.sgemm_kseq(A, B, transb, kblock=320))
+
+
+def test_port_dgemm_equals_kseq():
+    rng = np.random.default_rng(0)
+    for (M, N, K) in [(5, 5, 5), (22, 13, 32), (7, 6, 4), (32, 32, 32), (1, 9, 26)]:
+        A = rng.standard_normal((M, K))
+        B = rng.standard_normal((K, N))
+        assert np.array_equal(orc.port_dgemm(A, B), orc.dgemm_kseq(A, B, 0))
+
+
+def test_nt_reforder_close_to_kseq():
+    A, B = orc.gemm_inputs_f32(0, 80, 80, 80, 1)
+    r = orc.sgemm_nt_reforder(A, B)
+    k = orc.sgemm_kseq(A, B, 1)
+    # rows >= 5 of every strip use the k-sequential KERNEL5x16 order
+    assert np.array_equal(r[5:], k[5:])
+    ref = orc.sgemm_f64(A, B, 1)
+    ab = orc.sgemm_absprod(A, B, 1)
+    assert componentwise_err(r, ref, ab) <= fp32_bound(80)
+
+
+def test_dgemm_ld_oracle_accuracy():
+    rng = np.random.default_rng(1)
+    A = rng.standard_normal((20, 30)) * 1e3
+    B = rng.standard_normal((30, 10)) * 1e-3
+    ref = orc.dgemm_ld(A, B, 0)
+    assert normwise_err(ref, A @ B) < 1e-14
+
+
+def test_normal_scaled_generator():
+    x, s = orc.normal_scaled_f64(7, 10001)
+    assert 1e-3 <= s <= 1e3
+    z = x / s
+    assert abs(z.mean()) < 0.05 and abs(z.std() - 1) < 0.05
+    x2, s2 = orc.normal_scaled_f64(7, 10001)
+    assert np.array_equal(x, x2) and s == s2
+
+
+@pytest.mark.parametrize("path", sorted(glob.glob(os.path.join(GOLDEN, "*.npz"))))
+def test_golden_fixtures(path):
+    """Every committed fixture is reproduced by the oracle restatement named in
+    it (fixtures made by executing the reference's own instructions pin the
+    restatement; fixtures made by the oracle pin it against drift)."""
+    f = np.load(path)
+    kind = str(f["kind"])
+    A, B, C = f["A"], f["B"], f["C"]
+    if kind == "sgemm_nt_reforder":
+        got = orc.sgemm_nt_reforder(A, B)
+    elif kind == "sgemm_kseq_nn":
+        got = orc.sgemm_kseq(A, B, 0)
+    elif kind == "sgemm_kseq_nt":
+        got = orc.sgemm_kseq(A, B, 1)
+    elif kind == "dgemm_kseq_nn":
+        got = orc.dgemm_kseq(A, B, 0)
+    else:
+        pytest.fail(f"unknown fixture kind {kind}")
+    assert got.shape == C.shape
+    assert np.array_equal(got.view(np.uint8), np.ascontiguousarray(C).view(np.uint8)), kind
