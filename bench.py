@@ -52,7 +52,7 @@ def step_bytes(batch=BATCH):
 def parse():
     p = argparse.ArgumentParser()
     p.add_argument("--gpus", type=int, default=1)
-    p.add_argument("--steps", type=int, default=5)
+    p.add_argument("--steps", type=int, default=20)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="b200", choices=["b200", "reference"])
     p.add_argument("--mode", default="auto", choices=["auto", "fp32", "bf16x3", "bf16x6"])
@@ -174,7 +174,7 @@ class Clocks:
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
-                 "--format=csv,noheader,nounits", "-lms", "200"],
+                 "--format=csv,noheader,nounits", "-lms", "50"],
                 stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
         except (OSError, FileNotFoundError):
             self.proc = None
@@ -244,7 +244,7 @@ def run_gpu(args):
             ls.sgemm_batched_strided(tb, n, n, n, 1.0, A, n * n, B, n * n, 0.0, C, n * n, BATCH)
 
     # pick the mode: the fastest accurate one unless forced
-    candidates = [mode] if mode is not None else [ls.PREC_FP32, ls.PREC_BF16X6]
+    candidates = [mode] if mode is not None else [ls.PREC_FP32, ls.PREC_BF16X3, ls.PREC_BF16X6]
     results = {}
     for m in candidates:
         ls.set_precision(m)

@@ -1,13 +1,427 @@
-// ls_tc.cu -- split-BF16 GEMM on the sm_100a tensor cores (tcgen05 + TMEM).
+// ls_tc.cu -- split-BF16 SGEMM on the sm_100a tensor cores (tcgen05 + TMEM).
+//
+// Each FP32 input x is split into BF16 parts, x = hi + mid + lo (three parts,
+// 24 significant bits: LIBSHALOM_PREC_BF16X6) or x ~ hi + lo (two parts, 16
+// bits: LIBSHALOM_PREC_BF16X3).  C = A B is then a sum of BF16 products on the
+// tensor cores with FP32 accumulation in TMEM:
+//   D_main = sum A_hi B_hi
+//   D_corr = sum A_hi B_mid + A_mid B_hi + A_hi B_lo + A_lo B_hi + A_mid B_mid
+//            (bf16x3: A_hi B_lo + A_lo B_hi)
+// and C = alpha (D_main + D_corr) + beta C in the epilogue.  Keeping the
+// correction terms in their own accumulator keeps their rounding 2^-8 below
+// the main term's.
+//
+// The reference's "packing inside the micro-kernel" is the staging step here:
+// every K-slab of A and op(B) is read from row-major global memory by the
+// CTA's threads, split to BF16 in registers and written straight into shared
+// memory in the K-major core-matrix layout tcgen05.mma reads; there is no
+// separate packing pass and no packed copy in global memory.  Slab s+1 is
+// loaded into registers while the tensor core runs slab s; two shared-memory
+// buffers alternate, released by tcgen05.commit on an mbarrier.
+//
+// Small GEMMs (M <= 64) are packed G to a tile: the A rows of G GEMMs fill
+// the 128 rows of the MMA, their B columns sit side by side in its N, and
+// only the diagonal blocks of the 128 x N product are written back.
+#include <cuda_bf16.h>
+
+#include <algorithm>
+
 #include "ls_common.cuh"
 #include "ls_tc_launch.h"
+#include "ls_tc_ptx.cuh"
 
 namespace ls {
 
-int tc_sgemm_single(const GemmArgs<float> &, int, int) { return LIBSHALOM_ERR_UNSUPPORTED; }
-int tc_sgemm_strided(const GemmArgs<float> &, long, long, long, long, int) {
-  return LIBSHALOM_ERR_UNSUPPORTED;
+namespace {
+
+constexpr int TC_THREADS = 256;
+constexpr int TC_BM = 128;          // MMA M (TMEM lanes)
+constexpr int TC_BK = 32;           // K per slab (two MMA K-steps of 16)
+constexpr int TC_MAX_N = 128;       // MMA N per tile
+constexpr int TC_TMEM_COLS = 256;   // D_main (0..127) + D_corr (128..255)
+constexpr int SPLIT_BYTES = 16384;  // one split of one slab: A (8 KB) + B (8 KB)
+constexpr int BUF_BYTES = 3 * SPLIT_BYTES;
+constexpr int CHUNK_BYTES = 128 * 16;  // one 8-wide K chunk of 128 rows
+constexpr int TC_SMEM = 2 * BUF_BYTES + 64;
+
+struct TcProblem {
+  const float *A;
+  const float *B;
+  float *C;
+  long sA, sB, sC;  // element strides between consecutive GEMMs of the batch
+  int M, N, K;
+  int lda, ldb, ldc;
+  int transb;
+  float alpha, beta;
+  long count;      // GEMMs in the batch
+  int G;           // GEMMs packed per tile (block diagonal); 1 = tiled GEMM
+  int tile_n;      // MMA N of every tile (multiple of 16, <= 128)
+  int tiles_m, tiles_n;  // tiles per GEMM when G == 1
+  long num_tiles;
+  int nk;          // K slabs
+  int vec_a, vec_b;  // rows may be read with 16-byte vector loads
+  unsigned *err;   // device status word (bounded waits)
+};
+
+struct TileInfo {
+  long g0;   // first GEMM of the tile
+  int ng;    // GEMMs in the tile
+  int m0, n0;
+};
+
+__device__ __forceinline__ TileInfo decode_tile(const TcProblem &p, long t) {
+  TileInfo ti;
+  if (p.G > 1) {
+    ti.g0 = t * p.G;
+    ti.ng = (int)min((long)p.G, p.count - ti.g0);
+    ti.m0 = 0;
+    ti.n0 = 0;
+  } else {
+    const long per = (long)p.tiles_m * p.tiles_n;
+    ti.g0 = t / per;
+    const int r = (int)(t % per);
+    ti.ng = 1;
+    ti.m0 = (r / p.tiles_n) * TC_BM;
+    ti.n0 = (r % p.tiles_n) * p.tile_n;
+  }
+  return ti;
 }
+
+// split 8 floats into hi / mid / lo BF16 (packed pairs, element 0 in the low half)
+template <int NSPLIT>
+__device__ __forceinline__ void split8(const float *x, uint4 &h, uint4 &m, uint4 &l) {
+  uint32_t hh[4], mm[4], ll[4];
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const float x0 = x[2 * i], x1 = x[2 * i + 1];
+    __nv_bfloat162 b = __floats2bfloat162_rn(x0, x1);
+    const float r0 = x0 - __low2float(b), r1 = x1 - __high2float(b);
+    __nv_bfloat162 c = __floats2bfloat162_rn(r0, r1);
+    hh[i] = *reinterpret_cast<uint32_t *>(&b);
+    mm[i] = *reinterpret_cast<uint32_t *>(&c);
+    if (NSPLIT == 3) {
+      const float s0 = r0 - __low2float(c), s1 = r1 - __high2float(c);
+      __nv_bfloat162 d = __floats2bfloat162_rn(s0, s1);
+      ll[i] = *reinterpret_cast<uint32_t *>(&d);
+    } else {
+      ll[i] = 0;
+    }
+  }
+  h = make_uint4(hh[0], hh[1], hh[2], hh[3]);
+  m = make_uint4(mm[0], mm[1], mm[2], mm[3]);
+  l = make_uint4(ll[0], ll[1], ll[2], ll[3]);
+}
+
+// 8 consecutive floats of a row starting at column k0, zero past kend
+__device__ __forceinline__ void load_row8(const float *row, int k0, int kend, bool vec,
+                                          float *v) {
+  if (vec && k0 + 8 <= kend) {
+    const float4 a = __ldg(reinterpret_cast<const float4 *>(row + k0));
+    const float4 b = __ldg(reinterpret_cast<const float4 *>(row + k0 + 4));
+    v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w;
+    v[4] = b.x; v[5] = b.y; v[6] = b.z; v[7] = b.w;
+  } else {
+#pragma unroll
+    for (int t = 0; t < 8; ++t) v[t] = (k0 + t < kend) ? __ldg(row + k0 + t) : 0.0f;
+  }
+}
+
+template <int NSPLIT>
+__global__ void __launch_bounds__(TC_THREADS, 2) k_tc_sgemm(TcProblem p) {
+  extern __shared__ __align__(1024) unsigned char smem[];
+  uint64_t *bars = reinterpret_cast<uint64_t *>(smem + 2 * BUF_BYTES);  // [2]
+  uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(smem + 2 * BUF_BYTES + 16);
+  volatile int *s_abort = reinterpret_cast<volatile int *>(smem + 2 * BUF_BYTES + 20);
+
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const uint32_t smem_base = ptx::smem_u32(smem);
+
+  if (tid == 0) {
+    ptx::mbar_init(&bars[0], 1);
+    ptx::mbar_init(&bars[1], 1);
+    *s_abort = 0;
+    ptx::fence_mbar_init();
+  }
+  if (warp == 0) {
+    ptx::tmem_alloc(tmem_slot, TC_TMEM_COLS);
+    ptx::tmem_relinquish();
+  }
+  ptx::tc_fence_before();
+  __syncthreads();
+  ptx::tc_fence_after();
+  const uint32_t tmem = *tmem_slot;
+  const uint32_t idesc = ptx::idesc_bf16_f32(TC_BM, p.tile_n);
+
+  float ra[2][8], rb[2][8];
+  const int nb_items = p.tile_n * 4;  // B items (rows x 8-wide chunks)
+
+  // ---- global -> registers for slab s of tile ti ----
+  auto load_slab = [&](const TileInfo &ti, int s) {
+    const int k0 = s * TC_BK;
+#pragma unroll
+    for (int q = 0; q < 2; ++q) {
+      const int e = tid + q * TC_THREADS;  // 512 A items
+      const int r = e >> 2, c = e & 3;
+      int gi, i;
+      if (p.G > 1) { gi = r / p.M; i = r - gi * p.M; } else { gi = 0; i = ti.m0 + r; }
+      const bool ok = (p.G > 1) ? (gi < ti.ng) : (i < p.M);
+      if (ok) {
+        const float *row = p.A + (ti.g0 + gi) * p.sA + (long)i * p.lda;
+        load_row8(row, k0 + 8 * c, p.K, p.vec_a, ra[q]);
+      } else {
+#pragma unroll
+        for (int t = 0; t < 8; ++t) ra[q][t] = 0.0f;
+      }
+    }
+#pragma unroll
+    for (int q = 0; q < 2; ++q) {
+      const int e = tid + q * TC_THREADS;
+      int j, c;
+      if (p.transb) { j = e >> 2; c = e & 3; } else { j = e % p.tile_n; c = e / p.tile_n; }
+      bool ok = e < nb_items;
+      int gj = 0, jj = 0;
+      if (ok) {
+        if (p.G > 1) { gj = j / p.N; jj = j - gj * p.N; ok = gj < ti.ng; }
+        else { jj = ti.n0 + j; ok = jj < p.N; }
+      }
+      if (ok) {
+        const float *Bg = p.B + (ti.g0 + gj) * p.sB;
+        const int kk = k0 + 8 * c;
+        if (p.transb) {
+          load_row8(Bg + (long)jj * p.ldb, kk, p.K, p.vec_b, rb[q]);
+        } else {
+#pragma unroll
+          for (int t = 0; t < 8; ++t)
+            rb[q][t] = (kk + t < p.K) ? __ldg(Bg + (long)(kk + t) * p.ldb + jj) : 0.0f;
+        }
+      } else {
+#pragma unroll
+        for (int t = 0; t < 8; ++t) rb[q][t] = 0.0f;
+      }
+    }
+  };
+
+  // ---- registers -> split BF16 operands in buffer buf ----
+  auto store_slab = [&](int buf) {
+    unsigned char *base = smem + buf * BUF_BYTES;
+#pragma unroll
+    for (int q = 0; q < 2; ++q) {
+      const int e = tid + q * TC_THREADS;
+      const int r = e >> 2, c = e & 3;
+      uint4 h, m, l;
+      split8<NSPLIT>(ra[q], h, m, l);
+      const int off = c * CHUNK_BYTES + r * 16;
+      *reinterpret_cast<uint4 *>(base + off) = h;
+      *reinterpret_cast<uint4 *>(base + SPLIT_BYTES + off) = m;
+      if (NSPLIT == 3) *reinterpret_cast<uint4 *>(base + 2 * SPLIT_BYTES + off) = l;
+    }
+#pragma unroll
+    for (int q = 0; q < 2; ++q) {
+      const int e = tid + q * TC_THREADS;
+      if (e < nb_items) {
+        int j, c;
+        if (p.transb) { j = e >> 2; c = e & 3; } else { j = e % p.tile_n; c = e / p.tile_n; }
+        uint4 h, m, l;
+        split8<NSPLIT>(rb[q], h, m, l);
+        const int off = 8192 + c * CHUNK_BYTES + j * 16;
+        *reinterpret_cast<uint4 *>(base + off) = h;
+        *reinterpret_cast<uint4 *>(base + SPLIT_BYTES + off) = m;
+        if (NSPLIT == 3) *reinterpret_cast<uint4 *>(base + 2 * SPLIT_BYTES + off) = l;
+      }
+    }
+  };
+
+  long sc = 0;  // slabs issued by this CTA (selects buffer and mbarrier phase)
+  long t = blockIdx.x;
+  if (t < p.num_tiles) load_slab(decode_tile(p, t), 0);
+
+  for (; t < p.num_tiles; t += gridDim.x) {
+    const TileInfo ti = decode_tile(p, t);
+    for (int s = 0; s < p.nk; ++s, ++sc) {
+      const int buf = (int)(sc & 1);
+      bool ok = true;
+      if (sc >= 2) ok = ptx::mbar_wait_bounded(&bars[buf], (uint32_t)(((sc >> 1) - 1) & 1));
+      if (!ok) {
+        *s_abort = 1;
+        atomicOr(p.err, 1u);
+      } else {
+        store_slab(buf);
+      }
+      // prefetch the next slab (next K slab of this tile, or slab 0 of the next tile)
+      if (s + 1 < p.nk) load_slab(ti, s + 1);
+      else if (t + gridDim.x < p.num_tiles) load_slab(decode_tile(p, t + gridDim.x), 0);
+      ptx::fence_proxy_async_smem();
+      __syncthreads();
+      if (*s_abort) goto done;
+      if (tid == 0) {
+        ptx::tc_fence_after();
+        const uint32_t bb = smem_base + buf * BUF_BYTES;
+#pragma unroll
+        for (int ks = 0; ks < 2; ++ks) {
+          const uint32_t acc = (s > 0 || ks > 0) ? 1u : 0u;
+          uint64_t a[3], b[3];
+#pragma unroll
+          for (int sp = 0; sp < NSPLIT; ++sp) {
+            a[sp] = ptx::smem_desc(bb + sp * SPLIT_BYTES + ks * 2 * CHUNK_BYTES, CHUNK_BYTES, 128);
+            b[sp] = ptx::smem_desc(bb + sp * SPLIT_BYTES + 8192 + ks * 2 * CHUNK_BYTES,
+                                   CHUNK_BYTES, 128);
+          }
+          const uint32_t dm = tmem, dc = tmem + 128;
+          ptx::mma_bf16(dm, a[0], b[0], idesc, acc);
+          ptx::mma_bf16(dc, a[0], b[1], idesc, acc);
+          ptx::mma_bf16(dc, a[1], b[0], idesc, 1u);
+          if (NSPLIT == 3) {
+            ptx::mma_bf16(dc, a[0], b[2], idesc, 1u);
+            ptx::mma_bf16(dc, a[2], b[0], idesc, 1u);
+            ptx::mma_bf16(dc, a[1], b[1], idesc, 1u);
+          }
+        }
+        ptx::mma_commit(&bars[buf]);
+      }
+    }
+
+    // ---- epilogue: TMEM -> registers -> C ----
+    {
+      const long last = sc - 1;
+      const bool ok = ptx::mbar_wait_bounded(&bars[last & 1], (uint32_t)((last >> 1) & 1));
+      if (!ok) {
+        *s_abort = 1;
+        atomicOr(p.err, 1u);
+      }
+      ptx::tc_fence_after();
+      const int wq = warp & 3, wg = warp >> 2;
+      const int r = wq * 32 + lane;
+      int gi, i;
+      bool rok;
+      if (p.G > 1) { gi = r / p.M; i = r - gi * p.M; rok = gi < ti.ng; }
+      else { gi = 0; i = ti.m0 + r; rok = i < p.M; }
+      const int nch = p.tile_n / 8;
+      const int half = (nch + 1) / 2;
+      const int c_begin = wg ? half : 0, c_end = wg ? nch : half;
+      float *crow = p.C + (ti.g0 + gi) * p.sC + (long)i * p.ldc;
+      for (int ch = c_begin; ch < c_end; ++ch) {
+        float dm[8], dc[8];
+        const uint32_t ta = tmem + ((uint32_t)(wq * 32) << 16) + ch * 8;
+        ptx::tmem_ld8(ta, dm);
+        ptx::tmem_ld8(ta + 128, dc);
+        ptx::tmem_wait_ld();
+        if (!ok || !rok) continue;
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+          const int j = ch * 8 + u;
+          int jj;
+          bool cok;
+          if (p.G > 1) { const int gj = j / p.N; jj = j - gj * p.N; cok = gj == gi; }
+          else { jj = ti.n0 + j; cok = jj < p.N; }
+          if (cok) {
+            float v = p.alpha * (dm[u] + dc[u]);
+            if (p.beta != 0.0f) v = __fmaf_rn(p.beta, crow[jj], v);
+            crow[jj] = v;
+          }
+        }
+      }
+      ptx::tc_fence_before();
+      __syncthreads();
+      if (*s_abort) goto done;
+    }
+  }
+
+done:
+  __syncthreads();
+  if (*s_abort && sc > 0) {
+    // give MMAs still in flight a bounded chance to finish before freeing TMEM
+    ptx::mbar_wait_bounded(&bars[(sc - 1) & 1], (uint32_t)(((sc - 1) >> 1) & 1));
+  }
+  if (warp == 0) {
+    ptx::tc_fence_after();
+    ptx::tmem_dealloc(tmem, TC_TMEM_COLS);
+  }
+}
+
+// device status word for the bounded waits
+__device__ unsigned g_tc_err;
+
+int tc_launch(TcProblem &p, int mode) {
+  State &st = state();
+  void *errp = nullptr;
+  LS_CUDA_TRY(cudaGetSymbolAddress(&errp, g_tc_err));
+  p.err = reinterpret_cast<unsigned *>(errp);
+  const void *kern = mode == LIBSHALOM_PREC_BF16X6 ? (const void *)k_tc_sgemm<3>
+                                                   : (const void *)k_tc_sgemm<2>;
+  const int per_sm = std::min(2, occupancy_of(kern, TC_THREADS, TC_SMEM, 1));
+  const int grid = grid_for(p.num_tiles, per_sm);
+  if (mode == LIBSHALOM_PREC_BF16X6)
+    k_tc_sgemm<3><<<grid, TC_THREADS, TC_SMEM, st.stream>>>(p);
+  else
+    k_tc_sgemm<2><<<grid, TC_THREADS, TC_SMEM, st.stream>>>(p);
+  LS_CUDA_TRY(cudaGetLastError());
+  if (st.sync) {
+    // synchronous mode: report an expired device-side wait as a status
+    unsigned err = 0;
+    LS_CUDA_TRY(cudaStreamSynchronize(st.stream));
+    LS_CUDA_TRY(cudaMemcpyFromSymbol(&err, g_tc_err, sizeof(err)));
+    if (err) {
+      const unsigned zero = 0;
+      LS_CUDA_TRY(cudaMemcpyToSymbol(g_tc_err, &zero, sizeof(zero)));
+      return LIBSHALOM_ERR_DEVICE_TIMEOUT;
+    }
+  }
+  return LIBSHALOM_SUCCESS;
+}
+
+bool aligned16(const void *ptr) { return (reinterpret_cast<uintptr_t>(ptr) & 15) == 0; }
+
+void plan_tiles(TcProblem &p) {
+  if (p.M <= 64 && p.N <= 64) {
+    // block-diagonal packing of whole GEMMs into one 128-row tile
+    const int g_rows = TC_BM / p.M;
+    const int g_cols = TC_MAX_N / p.N;
+    p.G = std::max(1, std::min(g_rows, g_cols));
+    p.tile_n = std::min(TC_MAX_N, (int)cdiv((long)p.G * p.N, 16) * 16);
+    p.tiles_m = p.tiles_n = 1;
+    p.num_tiles = cdiv(p.count, p.G);
+  } else {
+    p.G = 1;
+    p.tile_n = std::min(TC_MAX_N, (int)cdiv(p.N, 16) * 16);
+    p.tiles_m = (int)cdiv(p.M, TC_BM);
+    p.tiles_n = (int)cdiv(p.N, p.tile_n);
+    p.num_tiles = (long)p.tiles_m * p.tiles_n * p.count;
+  }
+  p.nk = (int)std::max(1L, cdiv(p.K, TC_BK));
+}
+
+}  // namespace
+
+static bool tc_mode_ok(int mode) {
+  return mode == LIBSHALOM_PREC_BF16X3 || mode == LIBSHALOM_PREC_BF16X6;
+}
+
+int tc_sgemm_strided(const GemmArgs<float> &g, long sA, long sB, long sC, long count,
+                     int mode) {
+  if (!tc_mode_ok(mode)) return LIBSHALOM_ERR_INVALID_VALUE;
+  if (g.transa) return LIBSHALOM_ERR_UNSUPPORTED;
+  if (g.M > (1L << 30) || g.N > (1L << 30) || g.K > (1L << 30) || g.lda > INT32_MAX ||
+      g.ldb > INT32_MAX || g.ldc > INT32_MAX)
+    return LIBSHALOM_ERR_UNSUPPORTED;
+  TcProblem p{};
+  p.A = g.A; p.B = g.B; p.C = g.C;
+  p.sA = sA; p.sB = sB; p.sC = sC;
+  p.M = (int)g.M; p.N = (int)g.N; p.K = (int)g.K;
+  p.lda = (int)g.lda; p.ldb = (int)g.ldb; p.ldc = (int)g.ldc;
+  p.transb = g.transb;
+  p.alpha = g.alpha; p.beta = g.beta;
+  p.count = count;
+  p.vec_a = aligned16(g.A) && g.lda % 4 == 0 && sA % 4 == 0;
+  p.vec_b = aligned16(g.B) && g.ldb % 4 == 0 && sB % 4 == 0;
+  plan_tiles(p);
+  return tc_launch(p, mode);
+}
+
+int tc_sgemm_single(const GemmArgs<float> &g, int mode, int splits) {
+  (void)splits;
+  return tc_sgemm_strided(g, 0, 0, 0, 1, mode);
+}
+
 int tc_sgemm_grouped(const LibShalom_sgemm_entry *, long, int) {
   return LIBSHALOM_ERR_UNSUPPORTED;
 }
