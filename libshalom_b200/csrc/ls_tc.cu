@@ -60,6 +60,7 @@ struct TcProblem {
   long num_tiles;
   int nk;          // K slabs
   int vec_a, vec_b;  // rows may be read with 16-byte vector loads
+  int kc_slabs;    // DRAIN kernels: slabs per TMEM accumulation chunk
   unsigned *err;   // device status word (bounded waits)
 };
 
@@ -126,8 +127,13 @@ __device__ __forceinline__ void load_row8(const float *row, int k0, int kend, bo
   }
 }
 
-template <int NSPLIT>
-__global__ void __launch_bounds__(TC_THREADS, 2) k_tc_sgemm(TcProblem p) {
+// DRAIN: every p.kc_slabs K slabs the TMEM accumulators are added (round to
+// nearest) into FP32 registers and restarted.  The tensor core's FP32
+// accumulation truncates, so its error grows with the number of K steps it
+// accumulates; draining bounds that to kc_slabs * 2 steps (used for long-K
+// GEMMs).  The register sum costs 64 registers, hence one CTA per SM.
+template <int NSPLIT, bool DRAIN>
+__global__ void __launch_bounds__(TC_THREADS, DRAIN ? 1 : 2) k_tc_sgemm(TcProblem p) {
   extern __shared__ __align__(1024) unsigned char smem[];
   uint64_t *bars = reinterpret_cast<uint64_t *>(smem + 2 * BUF_BYTES);  // [2]
   uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(smem + 2 * BUF_BYTES + 16);
@@ -231,6 +237,34 @@ __global__ void __launch_bounds__(TC_THREADS, 2) k_tc_sgemm(TcProblem p) {
     }
   };
 
+  // epilogue geometry: warp quarter wq owns TMEM lanes 32*wq.., warpgroup wg
+  // owns one half of the 8-column chunks
+  const int wq = warp & 3, wg = warp >> 2;
+  const int nch = p.tile_n / 8;
+  const int half = (nch + 1) / 2;
+  const int c_begin = wg ? half : 0, c_end = wg ? nch : half;
+  constexpr int RMAX = DRAIN ? 64 : 1;  // register sum (DRAIN): 8 chunks x 8 columns
+  float R[RMAX];
+#pragma unroll
+  for (int u = 0; u < RMAX; ++u) R[u] = 0.0f;
+  auto fold_chunks = [&]() {
+    if constexpr (DRAIN) {
+#pragma unroll
+      for (int q = 0; q < 8; ++q) {
+        const int ch = c_begin + q;
+        if (ch < c_end) {
+          float dm[8], dc[8];
+          const uint32_t ta = tmem + ((uint32_t)(wq * 32) << 16) + ch * 8;
+          ptx::tmem_ld8(ta, dm);
+          ptx::tmem_ld8(ta + 128, dc);
+          ptx::tmem_wait_ld();
+#pragma unroll
+          for (int u = 0; u < 8; ++u) R[q * 8 + u] += dm[u] + dc[u];
+        }
+      }
+    }
+  };
+
   long sc = 0;  // slabs issued by this CTA (selects buffer and mbarrier phase)
   long t = blockIdx.x;
   if (t < p.num_tiles) load_slab(decode_tile(p, t), 0);
@@ -258,7 +292,8 @@ __global__ void __launch_bounds__(TC_THREADS, 2) k_tc_sgemm(TcProblem p) {
         const uint32_t bb = smem_base + buf * BUF_BYTES;
 #pragma unroll
         for (int ks = 0; ks < 2; ++ks) {
-          const uint32_t acc = (s > 0 || ks > 0) ? 1u : 0u;
+          const int s_in = DRAIN ? s % p.kc_slabs : s;  // slab within the accumulation chunk
+          const uint32_t acc = (s_in > 0 || ks > 0) ? 1u : 0u;
           uint64_t a[3], b[3];
 #pragma unroll
           for (int sp = 0; sp < NSPLIT; ++sp) {
@@ -278,6 +313,19 @@ __global__ void __launch_bounds__(TC_THREADS, 2) k_tc_sgemm(TcProblem p) {
         }
         ptx::mma_commit(&bars[buf]);
       }
+      if (DRAIN && (s + 1) % p.kc_slabs == 0 && s + 1 < p.nk) {
+        // chunk boundary: fold the accumulators into the register sum
+        const bool ok2 = ptx::mbar_wait_bounded(&bars[buf], (uint32_t)((sc >> 1) & 1));
+        if (!ok2) {
+          *s_abort = 1;
+          atomicOr(p.err, 1u);
+        }
+        ptx::tc_fence_after();
+        fold_chunks();
+        ptx::tc_fence_before();
+        __syncthreads();
+        if (*s_abort) goto done;
+      }
     }
 
     // ---- epilogue: TMEM -> registers -> C ----
@@ -289,23 +337,13 @@ __global__ void __launch_bounds__(TC_THREADS, 2) k_tc_sgemm(TcProblem p) {
         atomicOr(p.err, 1u);
       }
       ptx::tc_fence_after();
-      const int wq = warp & 3, wg = warp >> 2;
       const int r = wq * 32 + lane;
       int gi, i;
       bool rok;
       if (p.G > 1) { gi = r / p.M; i = r - gi * p.M; rok = gi < ti.ng; }
       else { gi = 0; i = ti.m0 + r; rok = i < p.M; }
-      const int nch = p.tile_n / 8;
-      const int half = (nch + 1) / 2;
-      const int c_begin = wg ? half : 0, c_end = wg ? nch : half;
       float *crow = p.C + (ti.g0 + gi) * p.sC + (long)i * p.ldc;
-      for (int ch = c_begin; ch < c_end; ++ch) {
-        float dm[8], dc[8];
-        const uint32_t ta = tmem + ((uint32_t)(wq * 32) << 16) + ch * 8;
-        ptx::tmem_ld8(ta, dm);
-        ptx::tmem_ld8(ta + 128, dc);
-        ptx::tmem_wait_ld();
-        if (!ok || !rok) continue;
+      auto store8 = [&](int ch, const float *v) {
 #pragma unroll
         for (int u = 0; u < 8; ++u) {
           const int j = ch * 8 + u;
@@ -314,10 +352,32 @@ __global__ void __launch_bounds__(TC_THREADS, 2) k_tc_sgemm(TcProblem p) {
           if (p.G > 1) { const int gj = j / p.N; jj = j - gj * p.N; cok = gj == gi; }
           else { jj = ti.n0 + j; cok = jj < p.N; }
           if (cok) {
-            float v = p.alpha * (dm[u] + dc[u]);
-            if (p.beta != 0.0f) v = __fmaf_rn(p.beta, crow[jj], v);
-            crow[jj] = v;
+            float x = p.alpha * v[u];
+            if (p.beta != 0.0f) x = __fmaf_rn(p.beta, crow[jj], x);
+            crow[jj] = x;
           }
+        }
+      };
+      if constexpr (DRAIN) {
+        fold_chunks();
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+          const int ch = c_begin + q;
+          if (ch < c_end && ok && rok) store8(ch, R + q * 8);
+        }
+#pragma unroll
+        for (int u = 0; u < RMAX; ++u) R[u] = 0.0f;
+      } else {
+        for (int ch = c_begin; ch < c_end; ++ch) {
+          float dm[8], dc[8];
+          const uint32_t ta = tmem + ((uint32_t)(wq * 32) << 16) + ch * 8;
+          ptx::tmem_ld8(ta, dm);
+          ptx::tmem_ld8(ta + 128, dc);
+          ptx::tmem_wait_ld();
+          if (!ok || !rok) continue;
+#pragma unroll
+          for (int u = 0; u < 8; ++u) dm[u] += dc[u];
+          store8(ch, dm);
         }
       }
       ptx::tc_fence_before();
@@ -346,14 +406,14 @@ int tc_launch(TcProblem &p, int mode) {
   void *errp = nullptr;
   LS_CUDA_TRY(cudaGetSymbolAddress(&errp, g_tc_err));
   p.err = reinterpret_cast<unsigned *>(errp);
-  const void *kern = mode == LIBSHALOM_PREC_BF16X6 ? (const void *)k_tc_sgemm<3>
-                                                   : (const void *)k_tc_sgemm<2>;
-  const int per_sm = std::min(2, occupancy_of(kern, TC_THREADS, TC_SMEM, 1));
+  const bool drain = p.nk > p.kc_slabs;
+  const void *kern = mode == LIBSHALOM_PREC_BF16X6
+                         ? (drain ? (const void *)k_tc_sgemm<3, true> : (const void *)k_tc_sgemm<3, false>)
+                         : (drain ? (const void *)k_tc_sgemm<2, true> : (const void *)k_tc_sgemm<2, false>);
+  const int per_sm = std::min(drain ? 1 : 2, occupancy_of(kern, TC_THREADS, TC_SMEM, 1));
   const int grid = grid_for(p.num_tiles, per_sm);
-  if (mode == LIBSHALOM_PREC_BF16X6)
-    k_tc_sgemm<3><<<grid, TC_THREADS, TC_SMEM, st.stream>>>(p);
-  else
-    k_tc_sgemm<2><<<grid, TC_THREADS, TC_SMEM, st.stream>>>(p);
+  void *args[] = {&p};
+  LS_CUDA_TRY(cudaLaunchKernel(kern, dim3(grid), dim3(TC_THREADS), args, TC_SMEM, st.stream));
   LS_CUDA_TRY(cudaGetLastError());
   if (st.sync) {
     // synchronous mode: report an expired device-side wait as a status
@@ -388,6 +448,7 @@ void plan_tiles(TcProblem &p) {
     p.num_tiles = (long)p.tiles_m * p.tiles_n * p.count;
   }
   p.nk = (int)std::max(1L, cdiv(p.K, TC_BK));
+  p.kc_slabs = 128 / TC_BK;  // TMEM accumulation chunk: 128 values of K
 }
 
 }  // namespace
