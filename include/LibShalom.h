@@ -164,6 +164,22 @@ LIBSHALOM_API int LibShalom_sgemm_batched_strided(int transb, long M, long N, lo
                                     const float *B, long strideB, float beta,
                                     float *C, long strideC, long count);
 
+/* Split-K SGEMM that allocates nothing.  No counterpart in the reference.
+ * For callers that cannot allocate device memory (their GPU memory is owned
+ * by another allocator, or a cudaMalloc in the middle of a call is not
+ * acceptable): same math and rounding order per K slice as
+ * LibShalom_sgemm_mp with LibShalom_set_splitk(splits), precision always
+ * plain FP32, but the partial sums live in a fixed array compiled into the
+ * library (LIBSHALOM_NOALLOC_SCRATCH_FLOATS floats, held on every GPU that
+ * loads the library until exit).  Returns LIBSHALOM_ERR_INVALID_VALUE, and
+ * launches nothing, when splits * M * N exceeds that size.  The first call
+ * on a device looks up the array's device address; make it before any stream
+ * capture.  All calls share the array: calls that overlap on the GPU race. */
+#define LIBSHALOM_NOALLOC_SCRATCH_FLOATS (2L * 1024 * 1024) /* 8 MiB */
+LIBSHALOM_API int LibShalom_sgemm_mp_noalloc(int transa, int transb, float *C, const float *A,
+                                             const float *B, long M, long N, long K,
+                                             int splits);
+
 /* Grouped DGEMM (same rules as LibShalom_sgemm_batched; FP64 FMA). */
 LIBSHALOM_API int LibShalom_dgemm_batched(const LibShalom_dgemm_entry *entries, long count);
 

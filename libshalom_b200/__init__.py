@@ -46,7 +46,7 @@ EXPORTED = (
     "LibShalom_set_precision", "LibShalom_get_precision", "LibShalom_set_splitk",
     "LibShalom_finalize",
     "LibShalom_sgemm_batched", "LibShalom_sgemm_batched_strided",
-    "LibShalom_dgemm_batched",
+    "LibShalom_dgemm_batched", "LibShalom_sgemm_mp_noalloc",
 )
 
 _L = ctypes.c_long
@@ -96,6 +96,7 @@ _SIGS = {
     "LibShalom_sgemm_batched_strided": (_I, [_I, _L, _L, _L, _F, _P, _L, _P, _L, _F, _P, _L,
                                              _L]),
     "LibShalom_dgemm_batched": (_I, [_P, _L]),
+    "LibShalom_sgemm_mp_noalloc": (_I, [_I, _I, _P, _P, _P, _L, _L, _L, _I]),
 }
 
 _lib = None
@@ -241,6 +242,20 @@ def dgemm_batched(entries_dev, count: int, check=True) -> int:
     st = lib().LibShalom_dgemm_batched(_ptr(entries_dev), int(count))
     if check:
         _check(st, "LibShalom_dgemm_batched")
+    return st
+
+
+NOALLOC_SCRATCH_FLOATS = 2 * 1024 * 1024
+
+
+def sgemm_mp_noalloc(transa, transb, C, A, B, M, N, K, splits, check=True) -> int:
+    """LibShalom_sgemm_mp_noalloc: split-K SGEMM for callers that cannot
+    allocate device memory; partial sums live in the library's fixed
+    8 MiB device array (splits * M * N <= NOALLOC_SCRATCH_FLOATS)."""
+    st = lib().LibShalom_sgemm_mp_noalloc(transa, transb, _ptr(C), _ptr(A), _ptr(B), M, N, K,
+                                          int(splits))
+    if check:
+        _check(st, "LibShalom_sgemm_mp_noalloc")
     return st
 
 

@@ -333,6 +333,25 @@ int run_gemm(const GemmArgs<T> &g, const SimtOptions &opt, SimtPlan *plan_out) {
   return LIBSHALOM_SUCCESS;
 }
 
+// Split-K GEMM whose partial sums live in a caller-provided device buffer of
+// at least splits * M * N floats; allocates nothing.
+int run_gemm_splitk_external(const GemmArgs<float> &g, int splits, float *partial) {
+  State &st = state();
+  int ncfg;
+  const CfgInfo *cfgs = Dispatch<float>::cfgs(&ncfg);
+  const int cfg = pick_cfg(cfgs, ncfg, g.M, g.N, g.K, st.num_sms, st.thread_cap);
+  long kchunk = cdiv(cdiv(g.K, splits), 320) * 320;  // keep GEMM_K blocks aligned
+  const int used = (int)cdiv(g.K, kchunk);
+  int rc = Dispatch<float>::single(cfg, g, used, kchunk, partial, 0, 0, true);
+  if (rc || used == 1) return rc;  // one slice: the tile kernel wrote C itself
+  const long total = g.M * g.N;
+  const int grid = (int)std::min<long>(cdiv(total, 256), (long)st.num_sms * 8);
+  k_splitk_reduce<float><<<std::max(grid, 1), 256, 0, st.stream>>>(partial, used, g.M, g.N,
+                                                                  g.C, g.ldc, g.alpha, g.beta);
+  LS_CUDA_TRY(cudaGetLastError());
+  return LIBSHALOM_SUCCESS;
+}
+
 template int run_gemm<float>(const GemmArgs<float> &, const SimtOptions &, SimtPlan *);
 template int run_gemm<double>(const GemmArgs<double> &, const SimtOptions &, SimtPlan *);
 
