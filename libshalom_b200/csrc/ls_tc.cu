@@ -12,12 +12,13 @@
 // the main term's.
 //
 // The reference's "packing inside the micro-kernel" is the staging step here:
-// every K-slab of A and op(B) is read from row-major global memory by the
-// CTA's threads, split to BF16 in registers and written straight into shared
-// memory in the K-major core-matrix layout tcgen05.mma reads; there is no
-// separate packing pass and no packed copy in global memory.  Slab s+1 is
-// loaded into registers while the tensor core runs slab s; two shared-memory
-// buffers alternate, released by tcgen05.commit on an mbarrier.
+// every K-slab of A and op(B) goes from row-major global memory into a ring of
+// FP32 shared-memory stages with cp.async (issued STAGES-1 slabs ahead, so
+// HBM keeps a deep queue of requests while the CTA converts and multiplies),
+// is split to BF16 by the CTA's threads and written in the K-major
+// core-matrix layout tcgen05.mma reads.  There is no separate packing pass and
+// no packed copy in global memory.  Two BF16 operand buffers alternate,
+// released by tcgen05.commit on an mbarrier.
 //
 // Small GEMMs (M <= 64) are packed G to a tile: the A rows of G GEMMs fill
 // the 128 rows of the MMA, their B columns sit side by side in its N, and
@@ -39,10 +40,27 @@ constexpr int TC_BM = 128;          // MMA M (TMEM lanes)
 constexpr int TC_BK = 32;           // K per slab (two MMA K-steps of 16)
 constexpr int TC_MAX_N = 128;       // MMA N per tile
 constexpr int TC_TMEM_COLS = 256;   // D_main (0..127) + D_corr (128..255)
-constexpr int SPLIT_BYTES = 16384;  // one split of one slab: A (8 KB) + B (8 KB)
+constexpr int STAGES = 3;           // FP32 staging ring depth
+
+// BF16 operand buffers: [split][A | B][4 chunks of 8 k][128 rows][16 bytes]
+constexpr int SPLIT_BYTES = 16384;
 constexpr int BUF_BYTES = 3 * SPLIT_BYTES;
-constexpr int CHUNK_BYTES = 128 * 16;  // one 8-wide K chunk of 128 rows
-constexpr int TC_SMEM = 2 * BUF_BYTES + 64;
+constexpr int CHUNK_BYTES = 128 * 16;
+
+// FP32 staging stage: A as [128 rows][36 floats] (32 used, padded against
+// bank conflicts); B as [128 rows][36] when B is N x K (Trans) or
+// [32 k][132 floats] when B is K x N (NoTrans).
+constexpr int SA_PITCH = 36;
+constexpr int SBT_PITCH = 36;
+constexpr int SBN_PITCH = 132;
+constexpr int STAGE_A_BYTES = 128 * SA_PITCH * 4;  // 18432
+constexpr int STAGE_B_BYTES = 128 * SBT_PITCH * 4; // 18432 (>= 32 * 132 * 4 = 16896)
+constexpr int STAGE_BYTES = STAGE_A_BYTES + STAGE_B_BYTES;
+
+constexpr int OFF_BUF = 0;
+constexpr int OFF_STAGE = 2 * BUF_BYTES;                    // 98304
+constexpr int OFF_BAR = OFF_STAGE + STAGES * STAGE_BYTES;   // 208896
+constexpr int TC_SMEM = OFF_BAR + 64;                       // 208960
 
 struct TcProblem {
   const float *A;
@@ -59,7 +77,8 @@ struct TcProblem {
   int tiles_m, tiles_n;  // tiles per GEMM when G == 1
   long num_tiles;
   int nk;          // K slabs
-  int vec_a, vec_b;  // rows may be read with 16-byte vector loads
+  int vec_a, vec_b;  // 16-byte cp.async allowed for A / B rows
+  int vec_c;       // 16-byte stores allowed for C rows
   int kc_slabs;    // DRAIN kernels: slabs per TMEM accumulation chunk
   unsigned *err;   // device status word (bounded waits)
 };
@@ -113,31 +132,36 @@ __device__ __forceinline__ void split8(const float *x, uint4 &h, uint4 &m, uint4
   l = make_uint4(ll[0], ll[1], ll[2], ll[3]);
 }
 
-// 8 consecutive floats of a row starting at column k0, zero past kend
-__device__ __forceinline__ void load_row8(const float *row, int k0, int kend, bool vec,
-                                          float *v) {
-  if (vec && k0 + 8 <= kend) {
-    const float4 a = __ldg(reinterpret_cast<const float4 *>(row + k0));
-    const float4 b = __ldg(reinterpret_cast<const float4 *>(row + k0 + 4));
-    v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w;
-    v[4] = b.x; v[5] = b.y; v[6] = b.z; v[7] = b.w;
-  } else {
-#pragma unroll
-    for (int t = 0; t < 8; ++t) v[t] = (k0 + t < kend) ? __ldg(row + k0 + t) : 0.0f;
-  }
+// ---- cp.async (global -> shared), zero fill past src_bytes ----
+__device__ __forceinline__ void cp_async16(uint32_t saddr, const void *g, int src_bytes) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(saddr), "l"(g),
+               "r"(src_bytes)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async4(uint32_t saddr, const void *g, int src_bytes) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;" ::"r"(saddr), "l"(g),
+               "r"(src_bytes)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() {
+  asm volatile("cp.async.commit_group;" ::: "memory");
+}
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
 }
 
 // DRAIN: every p.kc_slabs K slabs the TMEM accumulators are added (round to
 // nearest) into FP32 registers and restarted.  The tensor core's FP32
 // accumulation truncates, so its error grows with the number of K steps it
 // accumulates; draining bounds that to kc_slabs * 2 steps (used for long-K
-// GEMMs).  The register sum costs 64 registers, hence one CTA per SM.
+// GEMMs).
 template <int NSPLIT, bool DRAIN>
-__global__ void __launch_bounds__(TC_THREADS, DRAIN ? 1 : 2) k_tc_sgemm(TcProblem p) {
+__global__ void __launch_bounds__(TC_THREADS, 1) k_tc_sgemm(TcProblem p) {
   extern __shared__ __align__(1024) unsigned char smem[];
-  uint64_t *bars = reinterpret_cast<uint64_t *>(smem + 2 * BUF_BYTES);  // [2]
-  uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(smem + 2 * BUF_BYTES + 16);
-  volatile int *s_abort = reinterpret_cast<volatile int *>(smem + 2 * BUF_BYTES + 20);
+  uint64_t *bars = reinterpret_cast<uint64_t *>(smem + OFF_BAR);  // [2]
+  uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(smem + OFF_BAR + 16);
+  volatile int *s_abort = reinterpret_cast<volatile int *>(smem + OFF_BAR + 20);
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const uint32_t smem_base = ptx::smem_u32(smem);
@@ -157,65 +181,106 @@ __global__ void __launch_bounds__(TC_THREADS, DRAIN ? 1 : 2) k_tc_sgemm(TcProble
   ptx::tc_fence_after();
   const uint32_t tmem = *tmem_slot;
   const uint32_t idesc = ptx::idesc_bf16_f32(TC_BM, p.tile_n);
+  const int tn = p.tile_n;
 
-  float ra[2][8], rb[2][8];
-  const int nb_items = p.tile_n * 4;  // B items (rows x 8-wide chunks)
-
-  // ---- global -> registers for slab s of tile ti ----
-  auto load_slab = [&](const TileInfo &ti, int s) {
+  // ---- producer: cp.async of slab s of tile ti into staging stage st ----
+  auto issue_slab = [&](const TileInfo &ti, int s, int st) {
     const int k0 = s * TC_BK;
+    const uint32_t sa = smem_base + OFF_STAGE + st * STAGE_BYTES;
+    const uint32_t sb = sa + STAGE_A_BYTES;
+    // A: 128 rows x 32 floats
+    if (p.vec_a) {
 #pragma unroll
-    for (int q = 0; q < 2; ++q) {
-      const int e = tid + q * TC_THREADS;  // 512 A items
-      const int r = e >> 2, c = e & 3;
-      int gi, i;
-      if (p.G > 1) { gi = r / p.M; i = r - gi * p.M; } else { gi = 0; i = ti.m0 + r; }
-      const bool ok = (p.G > 1) ? (gi < ti.ng) : (i < p.M);
-      if (ok) {
-        const float *row = p.A + (ti.g0 + gi) * p.sA + (long)i * p.lda;
-        load_row8(row, k0 + 8 * c, p.K, p.vec_a, ra[q]);
-      } else {
-#pragma unroll
-        for (int t = 0; t < 8; ++t) ra[q][t] = 0.0f;
+      for (int q = 0; q < 4; ++q) {
+        const int e = tid + q * TC_THREADS;  // 1024 chunks of 4 floats
+        const int r = e >> 3, c4 = (e & 7) * 4;
+        int gi, i;
+        if (p.G > 1) { gi = r / p.M; i = r - gi * p.M; } else { gi = 0; i = ti.m0 + r; }
+        const bool ok = ((p.G > 1) ? (gi < ti.ng) : (i < p.M)) && k0 + c4 < p.K;
+        const float *src = ok ? p.A + (ti.g0 + gi) * p.sA + (long)i * p.lda + k0 + c4 : p.A;
+        const int bytes = ok ? 4 * min(4, p.K - k0 - c4) : 0;
+        cp_async16(sa + (r * SA_PITCH + c4) * 4, src, bytes);
+      }
+    } else {
+      for (int e = tid; e < 128 * 32; e += TC_THREADS) {
+        const int r = e >> 5, k = e & 31;
+        int gi, i;
+        if (p.G > 1) { gi = r / p.M; i = r - gi * p.M; } else { gi = 0; i = ti.m0 + r; }
+        const bool ok = ((p.G > 1) ? (gi < ti.ng) : (i < p.M)) && k0 + k < p.K;
+        const float *src = ok ? p.A + (ti.g0 + gi) * p.sA + (long)i * p.lda + k0 + k : p.A;
+        cp_async4(sa + (r * SA_PITCH + k) * 4, src, ok ? 4 : 0);
       }
     }
+    if (p.transb) {
+      // B stored N x K: tn rows x 32 floats, like A
+      if (p.vec_b) {
 #pragma unroll
-    for (int q = 0; q < 2; ++q) {
-      const int e = tid + q * TC_THREADS;
-      int j, c;
-      if (p.transb) { j = e >> 2; c = e & 3; } else { j = e % p.tile_n; c = e / p.tile_n; }
-      bool ok = e < nb_items;
-      int gj = 0, jj = 0;
-      if (ok) {
-        if (p.G > 1) { gj = j / p.N; jj = j - gj * p.N; ok = gj < ti.ng; }
-        else { jj = ti.n0 + j; ok = jj < p.N; }
-      }
-      if (ok) {
-        const float *Bg = p.B + (ti.g0 + gj) * p.sB;
-        const int kk = k0 + 8 * c;
-        if (p.transb) {
-          load_row8(Bg + (long)jj * p.ldb, kk, p.K, p.vec_b, rb[q]);
-        } else {
-#pragma unroll
-          for (int t = 0; t < 8; ++t)
-            rb[q][t] = (kk + t < p.K) ? __ldg(Bg + (long)(kk + t) * p.ldb + jj) : 0.0f;
+        for (int q = 0; q < 4; ++q) {
+          const int e = tid + q * TC_THREADS;
+          if (e < tn * 8) {
+            const int j = e >> 3, c4 = (e & 7) * 4;
+            int gj, jj;
+            if (p.G > 1) { gj = j / p.N; jj = j - gj * p.N; } else { gj = 0; jj = ti.n0 + j; }
+            const bool ok = ((p.G > 1) ? (gj < ti.ng) : (jj < p.N)) && k0 + c4 < p.K;
+            const float *src =
+                ok ? p.B + (ti.g0 + gj) * p.sB + (long)jj * p.ldb + k0 + c4 : p.B;
+            const int bytes = ok ? 4 * min(4, p.K - k0 - c4) : 0;
+            cp_async16(sb + (j * SBT_PITCH + c4) * 4, src, bytes);
+          }
         }
       } else {
-#pragma unroll
-        for (int t = 0; t < 8; ++t) rb[q][t] = 0.0f;
+        for (int e = tid; e < tn * 32; e += TC_THREADS) {
+          const int j = e >> 5, k = e & 31;
+          int gj, jj;
+          if (p.G > 1) { gj = j / p.N; jj = j - gj * p.N; } else { gj = 0; jj = ti.n0 + j; }
+          const bool ok = ((p.G > 1) ? (gj < ti.ng) : (jj < p.N)) && k0 + k < p.K;
+          const float *src = ok ? p.B + (ti.g0 + gj) * p.sB + (long)jj * p.ldb + k0 + k : p.B;
+          cp_async4(sb + (j * SBT_PITCH + k) * 4, src, ok ? 4 : 0);
+        }
+      }
+    } else {
+      // B stored K x N: 32 k-rows x tn floats
+      if (p.vec_b) {
+        const int cpr = tn / 4;  // 16-byte chunks per k-row
+        for (int e = tid; e < 32 * cpr; e += TC_THREADS) {
+          const int kr = e / cpr, j = (e - kr * cpr) * 4;
+          int gj, jj;
+          if (p.G > 1) { gj = j / p.N; jj = j - gj * p.N; } else { gj = 0; jj = ti.n0 + j; }
+          const bool ok = ((p.G > 1) ? (gj < ti.ng) : (jj < p.N)) && k0 + kr < p.K;
+          const float *src = ok ? p.B + (ti.g0 + gj) * p.sB + (long)(k0 + kr) * p.ldb + jj : p.B;
+          const int bytes = ok ? 4 * min(4, p.N - jj) : 0;
+          cp_async16(sb + (kr * SBN_PITCH + j) * 4, src, bytes);
+        }
+      } else {
+        for (int e = tid; e < 32 * tn; e += TC_THREADS) {
+          const int kr = e / tn, j = e - kr * tn;
+          int gj, jj;
+          if (p.G > 1) { gj = j / p.N; jj = j - gj * p.N; } else { gj = 0; jj = ti.n0 + j; }
+          const bool ok = ((p.G > 1) ? (gj < ti.ng) : (jj < p.N)) && k0 + kr < p.K;
+          const float *src = ok ? p.B + (ti.g0 + gj) * p.sB + (long)(k0 + kr) * p.ldb + jj : p.B;
+          cp_async4(sb + (kr * SBN_PITCH + j) * 4, src, ok ? 4 : 0);
+        }
       }
     }
   };
 
-  // ---- registers -> split BF16 operands in buffer buf ----
-  auto store_slab = [&](int buf) {
-    unsigned char *base = smem + buf * BUF_BYTES;
+  // ---- converter: staging stage st -> split BF16 operands in buffer buf ----
+  auto convert_slab = [&](int st, int buf) {
+    const float *fa = reinterpret_cast<const float *>(smem + OFF_STAGE + st * STAGE_BYTES);
+    const float *fb = reinterpret_cast<const float *>(smem + OFF_STAGE + st * STAGE_BYTES +
+                                                      STAGE_A_BYTES);
+    unsigned char *base = smem + OFF_BUF + buf * BUF_BYTES;
 #pragma unroll
     for (int q = 0; q < 2; ++q) {
-      const int e = tid + q * TC_THREADS;
+      const int e = tid + q * TC_THREADS;  // 512 items: 128 rows x 4 chunks of 8 k
       const int r = e >> 2, c = e & 3;
+      float x[8];
+      const float4 u = *reinterpret_cast<const float4 *>(fa + r * SA_PITCH + 8 * c);
+      const float4 v = *reinterpret_cast<const float4 *>(fa + r * SA_PITCH + 8 * c + 4);
+      x[0] = u.x; x[1] = u.y; x[2] = u.z; x[3] = u.w;
+      x[4] = v.x; x[5] = v.y; x[6] = v.z; x[7] = v.w;
       uint4 h, m, l;
-      split8<NSPLIT>(ra[q], h, m, l);
+      split8<NSPLIT>(x, h, m, l);
       const int off = c * CHUNK_BYTES + r * 16;
       *reinterpret_cast<uint4 *>(base + off) = h;
       *reinterpret_cast<uint4 *>(base + SPLIT_BYTES + off) = m;
@@ -224,11 +289,22 @@ __global__ void __launch_bounds__(TC_THREADS, DRAIN ? 1 : 2) k_tc_sgemm(TcProble
 #pragma unroll
     for (int q = 0; q < 2; ++q) {
       const int e = tid + q * TC_THREADS;
-      if (e < nb_items) {
+      if (e < tn * 4) {
         int j, c;
-        if (p.transb) { j = e >> 2; c = e & 3; } else { j = e % p.tile_n; c = e / p.tile_n; }
+        float x[8];
+        if (p.transb) {
+          j = e >> 2; c = e & 3;
+          const float4 u = *reinterpret_cast<const float4 *>(fb + j * SBT_PITCH + 8 * c);
+          const float4 v = *reinterpret_cast<const float4 *>(fb + j * SBT_PITCH + 8 * c + 4);
+          x[0] = u.x; x[1] = u.y; x[2] = u.z; x[3] = u.w;
+          x[4] = v.x; x[5] = v.y; x[6] = v.z; x[7] = v.w;
+        } else {
+          j = e % tn; c = e / tn;
+#pragma unroll
+          for (int t = 0; t < 8; ++t) x[t] = fb[(8 * c + t) * SBN_PITCH + j];
+        }
         uint4 h, m, l;
-        split8<NSPLIT>(rb[q], h, m, l);
+        split8<NSPLIT>(x, h, m, l);
         const int off = 8192 + c * CHUNK_BYTES + j * 16;
         *reinterpret_cast<uint4 *>(base + off) = h;
         *reinterpret_cast<uint4 *>(base + SPLIT_BYTES + off) = m;
@@ -240,7 +316,7 @@ __global__ void __launch_bounds__(TC_THREADS, DRAIN ? 1 : 2) k_tc_sgemm(TcProble
   // epilogue geometry: warp quarter wq owns TMEM lanes 32*wq.., warpgroup wg
   // owns one half of the 8-column chunks
   const int wq = warp & 3, wg = warp >> 2;
-  const int nch = p.tile_n / 8;
+  const int nch = tn / 8;
   const int half = (nch + 1) / 2;
   const int c_begin = wg ? half : 0, c_end = wg ? nch : half;
   constexpr int RMAX = DRAIN ? 64 : 1;  // register sum (DRAIN): 8 chunks x 8 columns
@@ -265,34 +341,46 @@ __global__ void __launch_bounds__(TC_THREADS, DRAIN ? 1 : 2) k_tc_sgemm(TcProble
     }
   };
 
-  long sc = 0;  // slabs issued by this CTA (selects buffer and mbarrier phase)
-  long t = blockIdx.x;
-  if (t < p.num_tiles) load_slab(decode_tile(p, t), 0);
+  // producer cursor (tile tp, slab spp), STAGES-1 slabs ahead of the consumer
+  long tp = blockIdx.x;
+  int spp = 0;
+  auto produce_next = [&](int st) {
+    if (tp < p.num_tiles) issue_slab(decode_tile(p, tp), spp, st);
+    cp_async_commit();  // empty groups keep the group count uniform
+    if (++spp == p.nk) { spp = 0; tp += gridDim.x; }
+  };
+#pragma unroll
+  for (int i = 0; i < STAGES - 1; ++i) produce_next(i);
 
-  for (; t < p.num_tiles; t += gridDim.x) {
+  long sc = 0;  // slabs consumed by this CTA (selects stage, buffer and mbarrier phase)
+  for (long t = blockIdx.x; t < p.num_tiles; t += gridDim.x) {
     const TileInfo ti = decode_tile(p, t);
     for (int s = 0; s < p.nk; ++s, ++sc) {
       const int buf = (int)(sc & 1);
+      const int st = (int)(sc % STAGES);
+      cp_async_wait<STAGES - 2>();  // this thread's copies of slab sc have landed
+      __syncthreads();              // ... and everyone else's
       bool ok = true;
       if (sc >= 2) ok = ptx::mbar_wait_bounded(&bars[buf], (uint32_t)(((sc >> 1) - 1) & 1));
       if (!ok) {
         *s_abort = 1;
         atomicOr(p.err, 1u);
       } else {
-        store_slab(buf);
+        convert_slab(st, buf);
       }
-      // prefetch the next slab (next K slab of this tile, or slab 0 of the next tile)
-      if (s + 1 < p.nk) load_slab(ti, s + 1);
-      else if (t + gridDim.x < p.num_tiles) load_slab(decode_tile(p, t + gridDim.x), 0);
+      // refill the stage consumed one slab ago (every thread is past its conversion)
+      produce_next((int)((sc + STAGES - 1) % STAGES));
       ptx::fence_proxy_async_smem();
       __syncthreads();
       if (*s_abort) goto done;
       if (tid == 0) {
         ptx::tc_fence_after();
-        const uint32_t bb = smem_base + buf * BUF_BYTES;
+        const uint32_t bb = smem_base + OFF_BUF + buf * BUF_BYTES;
+        const int s_in = DRAIN ? s % p.kc_slabs : s;  // slab within the accumulation chunk
+        const int ksteps = min(2, (p.K - s * TC_BK + 15) / 16);
 #pragma unroll
         for (int ks = 0; ks < 2; ++ks) {
-          const int s_in = DRAIN ? s % p.kc_slabs : s;  // slab within the accumulation chunk
+          if (ks >= ksteps) break;
           const uint32_t acc = (s_in > 0 || ks > 0) ? 1u : 0u;
           uint64_t a[3], b[3];
 #pragma unroll
@@ -338,23 +426,50 @@ __global__ void __launch_bounds__(TC_THREADS, DRAIN ? 1 : 2) k_tc_sgemm(TcProble
       }
       ptx::tc_fence_after();
       const int r = wq * 32 + lane;
-      int gi, i;
+      int gi, i, jlo, jhi;  // this row's GEMM, its row, and its valid tile columns
       bool rok;
-      if (p.G > 1) { gi = r / p.M; i = r - gi * p.M; rok = gi < ti.ng; }
-      else { gi = 0; i = ti.m0 + r; rok = i < p.M; }
-      float *crow = p.C + (ti.g0 + gi) * p.sC + (long)i * p.ldc;
+      if (p.G > 1) {
+        gi = r / p.M; i = r - gi * p.M; rok = gi < ti.ng;
+        jlo = gi * p.N; jhi = jlo + p.N;
+      } else {
+        gi = 0; i = ti.m0 + r; rok = i < p.M;
+        jlo = 0; jhi = min(tn, p.N - ti.n0);
+      }
+      rok = rok && ok;
+      float *crow = p.C + (ti.g0 + gi) * p.sC + (long)i * p.ldc + (ti.n0 - jlo);
+      // crow[j] is the C element of tile column j (j in [jlo, jhi))
+      const bool vec = p.vec_c && ((p.G == 1) || (p.N % 4 == 0));
       auto store8 = [&](int ch, const float *v) {
+        const int j0 = ch * 8;
+        if (!rok || j0 + 8 <= jlo || j0 >= jhi) return;
+        if (vec && j0 >= jlo && j0 + 8 <= jhi) {
+          float4 o0, o1;
+          if (p.beta != 0.0f) {
+            const float4 c0 = *reinterpret_cast<const float4 *>(crow + j0);
+            const float4 c1 = *reinterpret_cast<const float4 *>(crow + j0 + 4);
+            o0 = make_float4(__fmaf_rn(p.beta, c0.x, p.alpha * v[0]),
+                             __fmaf_rn(p.beta, c0.y, p.alpha * v[1]),
+                             __fmaf_rn(p.beta, c0.z, p.alpha * v[2]),
+                             __fmaf_rn(p.beta, c0.w, p.alpha * v[3]));
+            o1 = make_float4(__fmaf_rn(p.beta, c1.x, p.alpha * v[4]),
+                             __fmaf_rn(p.beta, c1.y, p.alpha * v[5]),
+                             __fmaf_rn(p.beta, c1.z, p.alpha * v[6]),
+                             __fmaf_rn(p.beta, c1.w, p.alpha * v[7]));
+          } else {
+            o0 = make_float4(p.alpha * v[0], p.alpha * v[1], p.alpha * v[2], p.alpha * v[3]);
+            o1 = make_float4(p.alpha * v[4], p.alpha * v[5], p.alpha * v[6], p.alpha * v[7]);
+          }
+          *reinterpret_cast<float4 *>(crow + j0) = o0;
+          *reinterpret_cast<float4 *>(crow + j0 + 4) = o1;
+        } else {
 #pragma unroll
-        for (int u = 0; u < 8; ++u) {
-          const int j = ch * 8 + u;
-          int jj;
-          bool cok;
-          if (p.G > 1) { const int gj = j / p.N; jj = j - gj * p.N; cok = gj == gi; }
-          else { jj = ti.n0 + j; cok = jj < p.N; }
-          if (cok) {
-            float x = p.alpha * v[u];
-            if (p.beta != 0.0f) x = __fmaf_rn(p.beta, crow[jj], x);
-            crow[jj] = x;
+          for (int u = 0; u < 8; ++u) {
+            const int j = j0 + u;
+            if (j >= jlo && j < jhi) {
+              float x = p.alpha * v[u];
+              if (p.beta != 0.0f) x = __fmaf_rn(p.beta, crow[j], x);
+              crow[j] = x;
+            }
           }
         }
       };
@@ -363,7 +478,7 @@ __global__ void __launch_bounds__(TC_THREADS, DRAIN ? 1 : 2) k_tc_sgemm(TcProble
 #pragma unroll
         for (int q = 0; q < 8; ++q) {
           const int ch = c_begin + q;
-          if (ch < c_end && ok && rok) store8(ch, R + q * 8);
+          if (ch < c_end) store8(ch, R + q * 8);
         }
 #pragma unroll
         for (int u = 0; u < RMAX; ++u) R[u] = 0.0f;
@@ -374,7 +489,6 @@ __global__ void __launch_bounds__(TC_THREADS, DRAIN ? 1 : 2) k_tc_sgemm(TcProble
           ptx::tmem_ld8(ta, dm);
           ptx::tmem_ld8(ta + 128, dc);
           ptx::tmem_wait_ld();
-          if (!ok || !rok) continue;
 #pragma unroll
           for (int u = 0; u < 8; ++u) dm[u] += dc[u];
           store8(ch, dm);
@@ -387,6 +501,7 @@ __global__ void __launch_bounds__(TC_THREADS, DRAIN ? 1 : 2) k_tc_sgemm(TcProble
   }
 
 done:
+  cp_async_wait<0>();  // no copy may still target shared memory when the CTA exits
   __syncthreads();
   if (*s_abort && sc > 0) {
     // give MMAs still in flight a bounded chance to finish before freeing TMEM
@@ -410,8 +525,8 @@ int tc_launch(TcProblem &p, int mode) {
   const void *kern = mode == LIBSHALOM_PREC_BF16X6
                          ? (drain ? (const void *)k_tc_sgemm<3, true> : (const void *)k_tc_sgemm<3, false>)
                          : (drain ? (const void *)k_tc_sgemm<2, true> : (const void *)k_tc_sgemm<2, false>);
-  const int per_sm = std::min(drain ? 1 : 2, occupancy_of(kern, TC_THREADS, TC_SMEM, 1));
-  const int grid = grid_for(p.num_tiles, per_sm);
+  (void)occupancy_of(kern, TC_THREADS, TC_SMEM, 1);  // raises the shared-memory limit
+  const int grid = grid_for(p.num_tiles, 1);
   void *args[] = {&p};
   LS_CUDA_TRY(cudaLaunchKernel(kern, dim3(grid), dim3(TC_THREADS), args, TC_SMEM, st.stream));
   LS_CUDA_TRY(cudaGetLastError());
@@ -472,9 +587,11 @@ int tc_sgemm_strided(const GemmArgs<float> &g, long sA, long sB, long sC, long c
   p.transb = g.transb;
   p.alpha = g.alpha; p.beta = g.beta;
   p.count = count;
-  p.vec_a = aligned16(g.A) && g.lda % 4 == 0 && sA % 4 == 0;
-  p.vec_b = aligned16(g.B) && g.ldb % 4 == 0 && sB % 4 == 0;
   plan_tiles(p);
+  p.vec_a = aligned16(g.A) && g.lda % 4 == 0 && sA % 4 == 0;
+  p.vec_b = aligned16(g.B) && g.ldb % 4 == 0 && sB % 4 == 0 &&
+            (g.transb || p.G == 1 || g.N % 4 == 0);
+  p.vec_c = aligned16(g.C) && g.ldc % 4 == 0 && sC % 4 == 0;
   return tc_launch(p, mode);
 }
 

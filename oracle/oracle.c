@@ -236,6 +236,41 @@ void orc_dgemm_kseq(int transb, long M, long N, long K, const double *A,
     }
 }
 
+/* DGEMM_NN rounding order (DGEMM_NN.c:5, driver at :2333).  Columns in the
+ * 6-wide strips and in the N4 tail block are k-sequential FMA chains
+ * (KERNEL7x6_*, EDGE_K_KERNEL7x6, N4 kernels).  The single trailing column
+ * of the N1 tail (N % 2 == 1, BEGIN_N1 at :3319) runs the KERNEL4x1/1x1
+ * kernels (:2265-2332): lane 0 accumulates even k, lane 1 odd k (fmul, then
+ * fmla over pairs of k), an odd last k is fmadd-ed into lane 0
+ * (EDGE_K_KERNEL1x1) and SAVE adds the lanes with faddp: C = s_even + s_odd.
+ * The N2 tail (N % 6 in {2,3}) is not restated: its output is wrong in the
+ * reference for several row tails (see the golden fixtures), and rows with
+ * M % 7 in {1,3,4} past 7*(M/7) are never written by the reference.  This
+ * function computes every element with the order of the path that covers its
+ * column. */
+void orc_dgemm_reforder(long M, long N, long K, const double *A,
+                        const double *B, double *C) {
+  const long n1col = (N % 2 == 1) ? N - 1 : -1;
+  for (long i = 0; i < M; ++i)
+    for (long j = 0; j < N; ++j) {
+      const double *a = A + i * K;
+      if (j == n1col && K >= 2) {
+        double s0 = a[0] * B[j], s1 = a[1] * B[N + j];
+        long k = 2;
+        for (; k + 1 < K; k += 2) {
+          s0 = fma(a[k], B[k * N + j], s0);
+          s1 = fma(a[k + 1], B[(k + 1) * N + j], s1);
+        }
+        if (k < K) s0 = fma(a[k], B[k * N + j], s0);
+        C[i * N + j] = s0 + s1;
+      } else {
+        double acc = a[0] * B[j];
+        for (long k = 1; k < K; ++k) acc = fma(a[k], B[k * N + j], acc);
+        C[i * N + j] = acc;
+      }
+    }
+}
+
 /* SGEMM_NT rounding order (test_SMM_NT.c:6 driver at :2181).  For every
  * 16-column strip (and the trailing 8-column strip), rows 0..4 run the
  * pack-fused PACK_KERNEL5x4_* kernels: lane l of the accumulator holds
@@ -513,6 +548,15 @@ void orc_dgemm_batched_ld(long count, const int *M, const int *N, const int *K,
       }
     g = e;
   }
+}
+
+/* correctly rounded fused multiply-add, element-wise (used by the AArch64
+ * interpreter in neon_emu.py to execute fmla / fmadd exactly) */
+void orc_fma_f32_vec(long n, const float *a, const float *b, const float *c, float *out) {
+  for (long i = 0; i < n; ++i) out[i] = fmaf(a[i], b[i], c[i]);
+}
+void orc_fma_f64_vec(long n, const double *a, const double *b, const double *c, double *out) {
+  for (long i = 0; i < n; ++i) out[i] = fma(a[i], b[i], c[i]);
 }
 
 int orc_max_threads(void) {

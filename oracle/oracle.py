@@ -53,6 +53,7 @@ def lib():
             "orc_sgemm_kseq": (None, [_I, _L, _L, _L, _f32p, _L, _f32p, _L, _f32p, _L, _L]),
             "orc_dgemm_kseq": (None, [_I, _L, _L, _L, _f64p, _L, _f64p, _L, _f64p, _L]),
             "orc_sgemm_nt_reforder": (None, [_L, _L, _L, _f32p, _f32p, _f32p]),
+            "orc_dgemm_reforder": (None, [_L, _L, _L, _f64p, _f64p, _f64p]),
             "orc_port_sgemm": (None, [_I, _L, _L, _L, _f32p, _L, _f32p, _L, _f32p, _L]),
             "orc_port_dgemm": (None, [_L, _L, _L, _f64p, _L, _f64p, _L, _f64p, _L, _I]),
             "orc_port_sgemm_mp": (None, [_I, _L, _L, _L, _f32p, _f32p, _f32p, _I]),
@@ -115,6 +116,14 @@ def gemm_inputs_f32(seed: int, M: int, N: int, K: int, transb: int):
     B = uniform_f32(seed, K * N, skip=M * K)
     B = B.reshape(N, K) if transb else B.reshape(K, N)
     return A, B
+
+
+def dgemm_inputs(seed: int, M: int, N: int, K: int):
+    """A (M x K) then B (K x N), each normal(0,1) * 10^u with its own u in
+    [-3, 3], from one drand48 stream (the batched-DGEMM workload's generator)."""
+    A, _ = normal_scaled_f64(seed, M * K)
+    B, _ = normal_scaled_f64(seed, K * N, skip=normal_scaled_draws(M * K))
+    return A.reshape(M, K), B.reshape(K, N)
 
 
 # --------------------------------------------------------------------------
@@ -182,6 +191,17 @@ def dgemm_kseq(A, B, transb, transa=0) -> np.ndarray:
     N = B.shape[0] if transb else B.shape[1]
     out = np.empty((M, N), np.float64)
     lib().orc_dgemm_kseq(int(transb), M, N, K, A, K, B, B.shape[1], out, N)
+    return out
+
+
+def dgemm_reforder(A, B) -> np.ndarray:
+    """DGEMM_NN's own rounding order (k-sequential, N1 tail lane-split)."""
+    A = _c(A, np.float64)
+    B = _c(B, np.float64)
+    M, K = A.shape
+    N = B.shape[1]
+    out = np.empty((M, N), np.float64)
+    lib().orc_dgemm_reforder(M, N, K, A, B, out)
     return out
 
 
