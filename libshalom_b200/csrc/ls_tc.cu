@@ -35,7 +35,7 @@ namespace ls {
 
 namespace {
 
-constexpr int TC_THREADS = 256;
+constexpr int TC_THREADS = 512;
 constexpr int TC_BM = 128;          // MMA M (TMEM lanes)
 constexpr int TC_BK = 32;           // K per slab (two MMA K-steps of 16)
 constexpr int TC_MAX_N = 128;       // MMA N per tile
@@ -183,25 +183,69 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_tc_sgemm(TcProblem p) {
   const uint32_t idesc = ptx::idesc_bf16_f32(TC_BM, p.tile_n);
   const int tn = p.tile_n;
 
-  // ---- producer: cp.async of slab s of tile ti into staging stage st ----
-  auto issue_slab = [&](const TileInfo &ti, int s, int st) {
+  // ---- per-thread assignments, constant over the kernel ----
+  // cp.async chunks (16-byte path): A and B (Trans) rows r0 and r0 + 64,
+  // 4-float chunk c4; B (NoTrans): k-row and column of chunks tid and tid + 512
+  const int r0 = tid >> 3, c4 = (tid & 7) * 4;
+  const int cpr = tn >> 2;  // 4-float chunks per k-row of a B (NoTrans) slab
+  int bn_kr[2], bn_j[2];
+  bool bn_on[2];
+#pragma unroll
+  for (int q = 0; q < 2; ++q) {
+    const int e = tid + q * TC_THREADS;
+    bn_on[q] = e < 32 * cpr;
+    bn_kr[q] = bn_on[q] ? e / cpr : 0;
+    bn_j[q] = bn_on[q] ? (e - bn_kr[q] * cpr) * 4 : 0;
+  }
+  // conversion items: A row cr, K chunk cc; B row/column bj, K chunk bc
+  const int cr = tid & 127, cc = tid >> 7;
+  const bool b_item = tid < 4 * tn;
+  const int bj = b_item ? tid % tn : 0, bc = b_item ? tid / tn : 0;
+
+  // producer state for its current tile: source rows of A and B
+  const float *a_src[2] = {nullptr, nullptr};
+  const float *b_src[2] = {nullptr, nullptr};
+  int b_cnt[2] = {0, 0};  // valid floats in a B (NoTrans) chunk
+  auto producer_tile = [&](long t) {
+    const TileInfo ti = decode_tile(p, t);
+#pragma unroll
+    for (int q = 0; q < 2; ++q) {
+      const int r = r0 + 64 * q;
+      int gi, i;
+      bool ok;
+      if (p.G > 1) { gi = r / p.M; i = r - gi * p.M; ok = gi < ti.ng; }
+      else { gi = 0; i = ti.m0 + r; ok = i < p.M; }
+      a_src[q] = ok ? p.A + (ti.g0 + gi) * p.sA + (long)i * p.lda : nullptr;
+      if (p.transb) {
+        int gj, jj;
+        if (p.G > 1) { gj = r / p.N; jj = r - gj * p.N; ok = r < tn && gj < ti.ng; }
+        else { gj = 0; jj = ti.n0 + r; ok = r < tn && jj < p.N; }
+        b_src[q] = ok ? p.B + (ti.g0 + gj) * p.sB + (long)jj * p.ldb : nullptr;
+      } else {
+        const int j = bn_j[q];
+        int gj, jj;
+        if (p.G > 1) { gj = j / p.N; jj = j - gj * p.N; ok = bn_on[q] && gj < ti.ng; }
+        else { gj = 0; jj = ti.n0 + j; ok = bn_on[q] && jj < p.N; }
+        b_src[q] = ok ? p.B + (ti.g0 + gj) * p.sB + jj : nullptr;
+        b_cnt[q] = ok ? min(4, p.N - jj) : 0;
+      }
+    }
+  };
+
+  // ---- producer: cp.async of slab s of the producer's tile into stage st ----
+  auto issue_slab = [&](long t, int s, int st) {
     const int k0 = s * TC_BK;
     const uint32_t sa = smem_base + OFF_STAGE + st * STAGE_BYTES;
     const uint32_t sb = sa + STAGE_A_BYTES;
-    // A: 128 rows x 32 floats
     if (p.vec_a) {
 #pragma unroll
-      for (int q = 0; q < 4; ++q) {
-        const int e = tid + q * TC_THREADS;  // 1024 chunks of 4 floats
-        const int r = e >> 3, c4 = (e & 7) * 4;
-        int gi, i;
-        if (p.G > 1) { gi = r / p.M; i = r - gi * p.M; } else { gi = 0; i = ti.m0 + r; }
-        const bool ok = ((p.G > 1) ? (gi < ti.ng) : (i < p.M)) && k0 + c4 < p.K;
-        const float *src = ok ? p.A + (ti.g0 + gi) * p.sA + (long)i * p.lda + k0 + c4 : p.A;
-        const int bytes = ok ? 4 * min(4, p.K - k0 - c4) : 0;
-        cp_async16(sa + (r * SA_PITCH + c4) * 4, src, bytes);
+      for (int q = 0; q < 2; ++q) {
+        const bool ok = a_src[q] != nullptr && k0 + c4 < p.K;
+        cp_async16(sa + ((r0 + 64 * q) * SA_PITCH + c4) * 4, ok ? a_src[q] + k0 + c4 : p.A,
+                   ok ? 4 * min(4, p.K - k0 - c4) : 0);
       }
     } else {
+      const TileInfo ti = decode_tile(p, t);
       for (int e = tid; e < 128 * 32; e += TC_THREADS) {
         const int r = e >> 5, k = e & 31;
         int gi, i;
@@ -211,24 +255,30 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_tc_sgemm(TcProblem p) {
         cp_async4(sa + (r * SA_PITCH + k) * 4, src, ok ? 4 : 0);
       }
     }
-    if (p.transb) {
-      // B stored N x K: tn rows x 32 floats, like A
-      if (p.vec_b) {
+    if (p.vec_b) {
+      if (p.transb) {
 #pragma unroll
-        for (int q = 0; q < 4; ++q) {
-          const int e = tid + q * TC_THREADS;
-          if (e < tn * 8) {
-            const int j = e >> 3, c4 = (e & 7) * 4;
-            int gj, jj;
-            if (p.G > 1) { gj = j / p.N; jj = j - gj * p.N; } else { gj = 0; jj = ti.n0 + j; }
-            const bool ok = ((p.G > 1) ? (gj < ti.ng) : (jj < p.N)) && k0 + c4 < p.K;
-            const float *src =
-                ok ? p.B + (ti.g0 + gj) * p.sB + (long)jj * p.ldb + k0 + c4 : p.B;
-            const int bytes = ok ? 4 * min(4, p.K - k0 - c4) : 0;
-            cp_async16(sb + (j * SBT_PITCH + c4) * 4, src, bytes);
+        for (int q = 0; q < 2; ++q) {
+          if (r0 + 64 * q < tn) {
+            const bool ok = b_src[q] != nullptr && k0 + c4 < p.K;
+            cp_async16(sb + ((r0 + 64 * q) * SBT_PITCH + c4) * 4,
+                       ok ? b_src[q] + k0 + c4 : p.B, ok ? 4 * min(4, p.K - k0 - c4) : 0);
           }
         }
       } else {
+#pragma unroll
+        for (int q = 0; q < 2; ++q) {
+          if (bn_on[q]) {
+            const int kk = k0 + bn_kr[q];
+            const bool ok = b_src[q] != nullptr && kk < p.K;
+            cp_async16(sb + (bn_kr[q] * SBN_PITCH + bn_j[q]) * 4,
+                       ok ? b_src[q] + (long)kk * p.ldb : p.B, ok ? 4 * b_cnt[q] : 0);
+          }
+        }
+      }
+    } else {
+      const TileInfo ti = decode_tile(p, t);
+      if (p.transb) {
         for (int e = tid; e < tn * 32; e += TC_THREADS) {
           const int j = e >> 5, k = e & 31;
           int gj, jj;
@@ -236,20 +286,6 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_tc_sgemm(TcProblem p) {
           const bool ok = ((p.G > 1) ? (gj < ti.ng) : (jj < p.N)) && k0 + k < p.K;
           const float *src = ok ? p.B + (ti.g0 + gj) * p.sB + (long)jj * p.ldb + k0 + k : p.B;
           cp_async4(sb + (j * SBT_PITCH + k) * 4, src, ok ? 4 : 0);
-        }
-      }
-    } else {
-      // B stored K x N: 32 k-rows x tn floats
-      if (p.vec_b) {
-        const int cpr = tn / 4;  // 16-byte chunks per k-row
-        for (int e = tid; e < 32 * cpr; e += TC_THREADS) {
-          const int kr = e / cpr, j = (e - kr * cpr) * 4;
-          int gj, jj;
-          if (p.G > 1) { gj = j / p.N; jj = j - gj * p.N; } else { gj = 0; jj = ti.n0 + j; }
-          const bool ok = ((p.G > 1) ? (gj < ti.ng) : (jj < p.N)) && k0 + kr < p.K;
-          const float *src = ok ? p.B + (ti.g0 + gj) * p.sB + (long)(k0 + kr) * p.ldb + jj : p.B;
-          const int bytes = ok ? 4 * min(4, p.N - jj) : 0;
-          cp_async16(sb + (kr * SBN_PITCH + j) * 4, src, bytes);
         }
       } else {
         for (int e = tid; e < 32 * tn; e += TC_THREADS) {
@@ -265,68 +301,59 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_tc_sgemm(TcProblem p) {
   };
 
   // ---- converter: staging stage st -> split BF16 operands in buffer buf ----
+  // consecutive threads take consecutive rows: the 16-byte shared stores of a
+  // quarter warp cover 128 contiguous bytes (no bank conflicts)
   auto convert_slab = [&](int st, int buf) {
     const float *fa = reinterpret_cast<const float *>(smem + OFF_STAGE + st * STAGE_BYTES);
-    const float *fb = reinterpret_cast<const float *>(smem + OFF_STAGE + st * STAGE_BYTES +
-                                                      STAGE_A_BYTES);
+    const float *fb = fa + STAGE_A_BYTES / 4;
     unsigned char *base = smem + OFF_BUF + buf * BUF_BYTES;
-#pragma unroll
-    for (int q = 0; q < 2; ++q) {
-      const int e = tid + q * TC_THREADS;  // 512 items: 128 rows x 4 chunks of 8 k
-      const int r = e >> 2, c = e & 3;
+    {
       float x[8];
-      const float4 u = *reinterpret_cast<const float4 *>(fa + r * SA_PITCH + 8 * c);
-      const float4 v = *reinterpret_cast<const float4 *>(fa + r * SA_PITCH + 8 * c + 4);
+      const float4 u = *reinterpret_cast<const float4 *>(fa + cr * SA_PITCH + 8 * cc);
+      const float4 v = *reinterpret_cast<const float4 *>(fa + cr * SA_PITCH + 8 * cc + 4);
       x[0] = u.x; x[1] = u.y; x[2] = u.z; x[3] = u.w;
       x[4] = v.x; x[5] = v.y; x[6] = v.z; x[7] = v.w;
       uint4 h, m, l;
       split8<NSPLIT>(x, h, m, l);
-      const int off = c * CHUNK_BYTES + r * 16;
+      const int off = cc * CHUNK_BYTES + cr * 16;
       *reinterpret_cast<uint4 *>(base + off) = h;
       *reinterpret_cast<uint4 *>(base + SPLIT_BYTES + off) = m;
       if (NSPLIT == 3) *reinterpret_cast<uint4 *>(base + 2 * SPLIT_BYTES + off) = l;
     }
+    if (b_item) {
+      float x[8];
+      if (p.transb) {
+        const float4 u = *reinterpret_cast<const float4 *>(fb + bj * SBT_PITCH + 8 * bc);
+        const float4 v = *reinterpret_cast<const float4 *>(fb + bj * SBT_PITCH + 8 * bc + 4);
+        x[0] = u.x; x[1] = u.y; x[2] = u.z; x[3] = u.w;
+        x[4] = v.x; x[5] = v.y; x[6] = v.z; x[7] = v.w;
+      } else {
 #pragma unroll
-    for (int q = 0; q < 2; ++q) {
-      const int e = tid + q * TC_THREADS;
-      if (e < tn * 4) {
-        int j, c;
-        float x[8];
-        if (p.transb) {
-          j = e >> 2; c = e & 3;
-          const float4 u = *reinterpret_cast<const float4 *>(fb + j * SBT_PITCH + 8 * c);
-          const float4 v = *reinterpret_cast<const float4 *>(fb + j * SBT_PITCH + 8 * c + 4);
-          x[0] = u.x; x[1] = u.y; x[2] = u.z; x[3] = u.w;
-          x[4] = v.x; x[5] = v.y; x[6] = v.z; x[7] = v.w;
-        } else {
-          j = e % tn; c = e / tn;
-#pragma unroll
-          for (int t = 0; t < 8; ++t) x[t] = fb[(8 * c + t) * SBN_PITCH + j];
-        }
-        uint4 h, m, l;
-        split8<NSPLIT>(x, h, m, l);
-        const int off = 8192 + c * CHUNK_BYTES + j * 16;
-        *reinterpret_cast<uint4 *>(base + off) = h;
-        *reinterpret_cast<uint4 *>(base + SPLIT_BYTES + off) = m;
-        if (NSPLIT == 3) *reinterpret_cast<uint4 *>(base + 2 * SPLIT_BYTES + off) = l;
+        for (int t = 0; t < 8; ++t) x[t] = fb[(8 * bc + t) * SBN_PITCH + bj];
       }
+      uint4 h, m, l;
+      split8<NSPLIT>(x, h, m, l);
+      const int off = 8192 + bc * CHUNK_BYTES + bj * 16;
+      *reinterpret_cast<uint4 *>(base + off) = h;
+      *reinterpret_cast<uint4 *>(base + SPLIT_BYTES + off) = m;
+      if (NSPLIT == 3) *reinterpret_cast<uint4 *>(base + 2 * SPLIT_BYTES + off) = l;
     }
   };
 
-  // epilogue geometry: warp quarter wq owns TMEM lanes 32*wq.., warpgroup wg
-  // owns one half of the 8-column chunks
+  // epilogue geometry: warp quarter wq owns TMEM lanes 32*wq..; the four
+  // warpgroups wg own consecutive ranges of the 8-column chunks
   const int wq = warp & 3, wg = warp >> 2;
   const int nch = tn / 8;
-  const int half = (nch + 1) / 2;
-  const int c_begin = wg ? half : 0, c_end = wg ? nch : half;
-  constexpr int RMAX = DRAIN ? 64 : 1;  // register sum (DRAIN): 8 chunks x 8 columns
+  const int per = (nch + 3) / 4;
+  const int c_begin = min(nch, wg * per), c_end = min(nch, c_begin + per);
+  constexpr int RMAX = DRAIN ? 32 : 1;  // register sum (DRAIN): 4 chunks x 8 columns
   float R[RMAX];
 #pragma unroll
   for (int u = 0; u < RMAX; ++u) R[u] = 0.0f;
   auto fold_chunks = [&]() {
     if constexpr (DRAIN) {
 #pragma unroll
-      for (int q = 0; q < 8; ++q) {
+      for (int q = 0; q < 4; ++q) {
         const int ch = c_begin + q;
         if (ch < c_end) {
           float dm[8], dc[8];
@@ -344,10 +371,15 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_tc_sgemm(TcProblem p) {
   // producer cursor (tile tp, slab spp), STAGES-1 slabs ahead of the consumer
   long tp = blockIdx.x;
   int spp = 0;
+  if (tp < p.num_tiles) producer_tile(tp);
   auto produce_next = [&](int st) {
-    if (tp < p.num_tiles) issue_slab(decode_tile(p, tp), spp, st);
+    if (tp < p.num_tiles) issue_slab(tp, spp, st);
     cp_async_commit();  // empty groups keep the group count uniform
-    if (++spp == p.nk) { spp = 0; tp += gridDim.x; }
+    if (++spp == p.nk) {
+      spp = 0;
+      tp += gridDim.x;
+      if (tp < p.num_tiles) producer_tile(tp);
+    }
   };
 #pragma unroll
   for (int i = 0; i < STAGES - 1; ++i) produce_next(i);
@@ -476,7 +508,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_tc_sgemm(TcProblem p) {
       if constexpr (DRAIN) {
         fold_chunks();
 #pragma unroll
-        for (int q = 0; q < 8; ++q) {
+        for (int q = 0; q < 4; ++q) {
           const int ch = c_begin + q;
           if (ch < c_end) store8(ch, R + q * 8);
         }
