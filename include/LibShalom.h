@@ -122,6 +122,13 @@ LIBSHALOM_API int LibShalom_get_precision(void);
  * (default), 1 = never split, s > 1 = split K into s slices. */
 LIBSHALOM_API int LibShalom_set_splitk(int splits);
 
+/* Operand staging of the tensor-core kernels: 1 (default) = TMA
+ * (cp.async.bulk.tensor) with warp-specialized producer / converter / MMA /
+ * epilogue warps whenever the operands are 16-byte aligned with 16-byte row
+ * strides; 0 = always the cp.async kernel (any alignment).  Results are the
+ * same either way. */
+LIBSHALOM_API int LibShalom_set_tma(int enable);
+
 /* Release the library's device workspace and cached plans. */
 LIBSHALOM_API void LibShalom_finalize(void);
 

@@ -44,6 +44,7 @@ EXPORTED = (
     "LibShalom_get_last_error", "LibShalom_error_string",
     "LibShalom_set_stream", "LibShalom_set_sync", "LibShalom_synchronize",
     "LibShalom_set_precision", "LibShalom_get_precision", "LibShalom_set_splitk",
+    "LibShalom_set_tma",
     "LibShalom_finalize",
     "LibShalom_sgemm_batched", "LibShalom_sgemm_batched_strided",
     "LibShalom_dgemm_batched", "LibShalom_sgemm_mp_noalloc",
@@ -91,6 +92,7 @@ _SIGS = {
     "LibShalom_set_precision": (_I, [_I]),
     "LibShalom_get_precision": (_I, []),
     "LibShalom_set_splitk": (_I, [_I]),
+    "LibShalom_set_tma": (_I, [_I]),
     "LibShalom_finalize": (None, []),
     "LibShalom_sgemm_batched": (_I, [_P, _L]),
     "LibShalom_sgemm_batched_strided": (_I, [_I, _L, _L, _L, _F, _P, _L, _P, _L, _F, _P, _L,
@@ -211,6 +213,11 @@ def get_precision() -> int:
 
 def set_splitk(splits: int) -> None:
     _check(lib().LibShalom_set_splitk(int(splits)), "LibShalom_set_splitk")
+
+
+def set_tma(on: bool) -> None:
+    """Tensor-core kernels: TMA warp-specialized variant (default) or cp.async."""
+    _check(lib().LibShalom_set_tma(1 if on else 0), "LibShalom_set_tma")
 
 
 def finalize() -> None:

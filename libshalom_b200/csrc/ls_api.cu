@@ -270,6 +270,13 @@ int LibShalom_set_splitk(int splits) {
   return rc;
 }
 
+int LibShalom_set_tma(int enable) {
+  std::lock_guard<std::mutex> lk(state().mu);
+  state().use_tma = enable != 0;
+  set_error(LIBSHALOM_SUCCESS);
+  return LIBSHALOM_SUCCESS;
+}
+
 void LibShalom_finalize(void) {
   std::lock_guard<std::mutex> lk(state().mu);
   State &st = state();

@@ -45,6 +45,9 @@ struct State {
   int ways_m = 0, ways_n = 0;  // LibShalom_set_thread_ways (one-shot)
   int precision = LIBSHALOM_PREC_FP32;
   int splitk = 0;
+  // tensor-core kernels: the TMA warp-specialized variant where the operands
+  // allow it (LIBSHALOM_NO_TMA=1 in the environment selects the cp.async one)
+  bool use_tma = true;
   // device workspace (split-K partials, work counters, work lists)
   void *ws = nullptr;
   size_t ws_bytes = 0;

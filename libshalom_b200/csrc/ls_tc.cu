@@ -23,6 +23,8 @@
 // Small GEMMs (M <= 64) are packed G to a tile: the A rows of G GEMMs fill
 // the 128 rows of the MMA, their B columns sit side by side in its N, and
 // only the diagonal blocks of the 128 x N product are written back.
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda_bf16.h>
 
 #include <algorithm>
@@ -545,8 +547,459 @@ done:
   }
 }
 
+// ===========================================================================
+// Warp-specialized TMA variant (operands that TMA can address: 16-byte
+// aligned bases and row strides).  Roles, all connected by mbarriers:
+//   warp 0      producer: one thread issues cp.async.bulk.tensor loads of the
+//               A and op(B) slabs into a 4-deep FP32 ring (A and B (Trans)
+//               boxes land 128-byte swizzled)
+//   warp 1      MMA: one thread issues tcgen05.mma into one of two TMEM
+//               accumulator sets (512 columns), so the epilogue of one tile or
+//               accumulation chunk overlaps the MMAs of the next
+//   warps 2-9   converters: FP32 slab -> split BF16 core matrices (2 buffers)
+//   warps 10-17 epilogue: TMEM -> registers -> C (and the register fold of the
+//               long-K chunks)
+// ===========================================================================
+constexpr int WS_WARPS = 18;
+constexpr int WS_THREADS = WS_WARPS * 32;
+constexpr int WS_STAGES = 4;
+constexpr int WS_STAGE_BYTES = 32768;                           // A 16 KB + B 16 KB
+constexpr int WS_OFF_BUF = 0;                                   // 2 BF16 operand buffers
+constexpr int WS_OFF_STAGE = 2 * BUF_BYTES;                     // 98304 (1024-aligned)
+constexpr int WS_OFF_BAR = WS_OFF_STAGE + WS_STAGES * WS_STAGE_BYTES;  // 229376
+constexpr int WS_SMEM = WS_OFF_BAR + 256;
+constexpr int W_CONV0 = 2, N_CONV = 8, W_EPI0 = 10, N_EPI = 8;
+constexpr int WS_TMEM_COLS = 512;  // 2 x (D_main 128 + D_corr 128)
+
+// mbarrier slots (8 bytes each) after WS_OFF_BAR
+enum { B_FULL = 0, B_EMPTY = 4, B_BFULL = 8, B_BEMPTY = 10, B_AFULL = 12, B_AEMPTY = 14,
+       B_FINAL = 16, B_COUNT = 17 };
+
+struct WsArgs {
+  TcProblem p;
+  uint32_t tx_bytes;  // A box + B box bytes per slab
+  int nn_w;           // B (NoTrans) box width in floats (row pitch of the staged slab)
+};
+
+__device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(ptx::smem_u32(bar)) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive_tx(uint64_t *bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%1], %0;" ::"r"(bytes),
+               "r"(ptx::smem_u32(bar))
+               : "memory");
+}
+__device__ __forceinline__ void tma_load_3d(uint32_t dst, const CUtensorMap *map, uint64_t *bar,
+                                            int c0, int c1, int c2) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes"
+      " [%0], [%1, {%3, %4, %5}], [%2];" ::"r"(dst),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(ptx::smem_u32(bar)), "r"(c0), "r"(c1), "r"(c2)
+      : "memory");
+}
+
+// Bounded wait that also gives up as soon as another role has aborted.
+__device__ __forceinline__ bool ws_wait(uint64_t *bar, uint32_t parity, volatile int *abort_flag,
+                                        unsigned *err) {
+  for (uint32_t it = 0; it < (1u << 22); ++it) {
+    if (ptx::mbar_try_wait(bar, parity)) return true;
+    if ((it & 255) == 255 && *abort_flag) return false;
+    if (it > 64) __nanosleep(it < 4096 ? 32 : 256);
+  }
+  *abort_flag = 1;
+  atomicOr(err, 1u);
+  return false;
+}
+
+template <int NSPLIT, bool DRAIN>
+__global__ void __launch_bounds__(WS_THREADS, 1)
+    k_tc_ws(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
+            const WsArgs args) {
+  extern __shared__ __align__(1024) unsigned char smem[];
+  const TcProblem &p = args.p;
+  uint64_t *bars = reinterpret_cast<uint64_t *>(smem + WS_OFF_BAR);
+  uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(smem + WS_OFF_BAR + 8 * B_COUNT);
+  volatile int *s_abort = reinterpret_cast<volatile int *>(smem + WS_OFF_BAR + 8 * B_COUNT + 4);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const uint32_t smem_base = ptx::smem_u32(smem);
+  const int tn = p.tile_n;
+  const int kc = DRAIN ? p.kc_slabs : (1 << 30);
+
+  if (tid == 0) {
+    for (int i = 0; i < WS_STAGES; ++i) {
+      ptx::mbar_init(&bars[B_FULL + i], 1);
+      ptx::mbar_init(&bars[B_EMPTY + i], N_CONV);
+    }
+    for (int i = 0; i < 2; ++i) {
+      ptx::mbar_init(&bars[B_BFULL + i], N_CONV);
+      ptx::mbar_init(&bars[B_BEMPTY + i], 1);
+      ptx::mbar_init(&bars[B_AFULL + i], 1);
+      ptx::mbar_init(&bars[B_AEMPTY + i], N_EPI);
+    }
+    ptx::mbar_init(&bars[B_FINAL], 1);
+    *s_abort = 0;
+    ptx::fence_mbar_init();
+  }
+  if (warp == 1) {
+    ptx::tmem_alloc(tmem_slot, WS_TMEM_COLS);
+    ptx::tmem_relinquish();
+  }
+  ptx::tc_fence_before();
+  __syncthreads();
+  ptx::tc_fence_after();
+  const uint32_t tmem = *tmem_slot;
+
+  if (warp == 0) {
+    // ------------------------------ producer ------------------------------
+    if (lane == 0) {
+      long j = 0;
+      for (long t = blockIdx.x; t < p.num_tiles && !*s_abort; t += gridDim.x) {
+        const TileInfo ti = decode_tile(p, t);
+        for (int s = 0; s < p.nk; ++s, ++j) {
+          const int st = (int)(j % WS_STAGES);
+          if (j >= WS_STAGES &&
+              !ws_wait(&bars[B_EMPTY + st], (uint32_t)(((j / WS_STAGES) - 1) & 1), s_abort, p.err))
+            break;
+          const uint32_t dst = smem_base + WS_OFF_STAGE + st * WS_STAGE_BYTES;
+          mbar_arrive_tx(&bars[B_FULL + st], args.tx_bytes);
+          const int k0 = s * TC_BK;
+          const int g = (int)ti.g0;
+          tma_load_3d(dst, &tmA, &bars[B_FULL + st], k0, ti.m0, g);
+          if (p.transb) tma_load_3d(dst + 16384, &tmB, &bars[B_FULL + st], k0, ti.n0, g);
+          else tma_load_3d(dst + 16384, &tmB, &bars[B_FULL + st], ti.n0, k0, g);
+        }
+      }
+    }
+  } else if (warp == 1) {
+    // -------------------------------- MMA ---------------------------------
+    if (lane == 0) {
+      const uint32_t idesc = ptx::idesc_bf16_f32(TC_BM, tn);
+      long j = 0, u = 0;
+      bool ok = true;
+      for (long t = blockIdx.x; ok && t < p.num_tiles; t += gridDim.x) {
+        for (int s = 0; ok && s < p.nk; ++s, ++j) {
+          const int s_in = s % kc;
+          if (s_in == 0) {
+            // new accumulation chunk: wait until the epilogue has drained this set
+            const int a = (int)(u & 1);
+            if (u >= 2 && !ws_wait(&bars[B_AEMPTY + a], (uint32_t)(((u >> 1) - 1) & 1), s_abort,
+                                   p.err)) {
+              ok = false;
+              break;
+            }
+          }
+          const int b = (int)(j & 1);
+          if (!ws_wait(&bars[B_BFULL + b], (uint32_t)((j >> 1) & 1), s_abort, p.err)) {
+            ok = false;
+            break;
+          }
+          ptx::tc_fence_after();
+          const uint32_t acc_base = tmem + (uint32_t)((u & 1) * 256);
+          const uint32_t bb = smem_base + WS_OFF_BUF + b * BUF_BYTES;
+          const int ksteps = min(2, (p.K - s * TC_BK + 15) / 16);
+#pragma unroll
+          for (int ks = 0; ks < 2; ++ks) {
+            if (ks >= ksteps) break;
+            const uint32_t acc = (s_in > 0 || ks > 0) ? 1u : 0u;
+            uint64_t da[3], db[3];
+#pragma unroll
+            for (int sp = 0; sp < NSPLIT; ++sp) {
+              da[sp] = ptx::smem_desc(bb + sp * SPLIT_BYTES + ks * 2 * CHUNK_BYTES, CHUNK_BYTES, 128);
+              db[sp] = ptx::smem_desc(bb + sp * SPLIT_BYTES + 8192 + ks * 2 * CHUNK_BYTES,
+                                      CHUNK_BYTES, 128);
+            }
+            ptx::mma_bf16(acc_base, da[0], db[0], idesc, acc);
+            ptx::mma_bf16(acc_base + 128, da[0], db[1], idesc, acc);
+            ptx::mma_bf16(acc_base + 128, da[1], db[0], idesc, 1u);
+            if (NSPLIT == 3) {
+              ptx::mma_bf16(acc_base + 128, da[0], db[2], idesc, 1u);
+              ptx::mma_bf16(acc_base + 128, da[2], db[0], idesc, 1u);
+              ptx::mma_bf16(acc_base + 128, da[1], db[1], idesc, 1u);
+            }
+          }
+          ptx::mma_commit(&bars[B_BEMPTY + b]);  // operand buffer b may be refilled
+          if (s_in == kc - 1 || s == p.nk - 1) {
+            ptx::mma_commit(&bars[B_AFULL + (u & 1)]);  // accumulation chunk complete
+            ++u;
+          }
+        }
+      }
+      // every MMA this thread issued has completed before TMEM is freed
+      ptx::mma_commit(&bars[B_FINAL]);
+      ptx::mbar_wait_bounded(&bars[B_FINAL], 0);
+    }
+  } else if (warp < W_EPI0) {
+    // ----------------------------- converters -----------------------------
+    const int ct = tid - W_CONV0 * 32;  // 0..255
+    const int cr = ct & 127, cc0 = ct >> 7;  // A rows cr, chunks cc0 and cc0 + 2
+    const bool nn = !p.transb;
+    const int nn_w = args.nn_w;
+    long j = 0;
+    bool ok = true;
+    for (long t = blockIdx.x; ok && t < p.num_tiles; t += gridDim.x) {
+      for (int s = 0; s < p.nk; ++s, ++j) {
+        const int st = (int)(j % WS_STAGES), b = (int)(j & 1);
+        if (!ws_wait(&bars[B_FULL + st], (uint32_t)((j / WS_STAGES) & 1), s_abort, p.err)) {
+          ok = false;
+          break;
+        }
+        if (j >= 2 && !ws_wait(&bars[B_BEMPTY + b], (uint32_t)(((j >> 1) - 1) & 1), s_abort,
+                               p.err)) {
+          ok = false;
+          break;
+        }
+        const unsigned char *stg = smem + WS_OFF_STAGE + st * WS_STAGE_BYTES;
+        unsigned char *base = smem + WS_OFF_BUF + b * BUF_BYTES;
+#pragma unroll
+        for (int q = 0; q < 2; ++q) {
+          // A: row cr, 8-float chunk c (16-byte chunks 2c, 2c+1, 128-byte swizzle)
+          const int c = cc0 + 2 * q;
+          const unsigned char *row = stg + cr * 128;
+          const float4 u0 = *reinterpret_cast<const float4 *>(row + (((2 * c) ^ (cr & 7)) << 4));
+          const float4 u1 =
+              *reinterpret_cast<const float4 *>(row + (((2 * c + 1) ^ (cr & 7)) << 4));
+          float x[8] = {u0.x, u0.y, u0.z, u0.w, u1.x, u1.y, u1.z, u1.w};
+          uint4 h, m, l;
+          split8<NSPLIT>(x, h, m, l);
+          const int off = c * CHUNK_BYTES + cr * 16;
+          *reinterpret_cast<uint4 *>(base + off) = h;
+          *reinterpret_cast<uint4 *>(base + SPLIT_BYTES + off) = m;
+          if (NSPLIT == 3) *reinterpret_cast<uint4 *>(base + 2 * SPLIT_BYTES + off) = l;
+        }
+#pragma unroll
+        for (int q = 0; q < 2; ++q) {
+          const int e = ct + q * 256;
+          if (e < 4 * tn) {
+            const int jj = e % tn, c = e / tn;
+            float x[8];
+            if (!nn) {
+              const unsigned char *row = stg + 16384 + jj * 128;
+              const float4 u0 =
+                  *reinterpret_cast<const float4 *>(row + (((2 * c) ^ (jj & 7)) << 4));
+              const float4 u1 =
+                  *reinterpret_cast<const float4 *>(row + (((2 * c + 1) ^ (jj & 7)) << 4));
+              x[0] = u0.x; x[1] = u0.y; x[2] = u0.z; x[3] = u0.w;
+              x[4] = u1.x; x[5] = u1.y; x[6] = u1.z; x[7] = u1.w;
+            } else {
+              // [g][32 k][nn_w] (packed) or [32 k][tn]: column jj of GEMM g = jj / N
+              const float *fb = reinterpret_cast<const float *>(stg + 16384);
+              int col = jj, gofs = 0;
+              if (p.G > 1) {
+                const int g = jj / p.N;
+                col = jj - g * p.N;
+                gofs = g * 32 * nn_w;
+              }
+#pragma unroll
+              for (int tk = 0; tk < 8; ++tk) x[tk] = fb[gofs + (8 * c + tk) * nn_w + col];
+            }
+            uint4 h, m, l;
+            split8<NSPLIT>(x, h, m, l);
+            const int off = 8192 + c * CHUNK_BYTES + jj * 16;
+            *reinterpret_cast<uint4 *>(base + off) = h;
+            *reinterpret_cast<uint4 *>(base + SPLIT_BYTES + off) = m;
+            if (NSPLIT == 3) *reinterpret_cast<uint4 *>(base + 2 * SPLIT_BYTES + off) = l;
+          }
+        }
+        ptx::fence_proxy_async_smem();
+        __syncwarp();
+        if (lane == 0) {
+          mbar_arrive(&bars[B_EMPTY + st]);  // staging slab consumed
+          mbar_arrive(&bars[B_BFULL + b]);   // operand buffer ready for the MMA
+        }
+      }
+    }
+  } else {
+    // ------------------------------ epilogue ------------------------------
+    const int wq = warp & 3, half = (warp - W_EPI0) >> 2;
+    const int r = wq * 32 + lane;
+    const int nch = tn / 8, per = (nch + 1) / 2;
+    const int c_begin = min(nch, half * per), c_end = min(nch, c_begin + per);
+    constexpr int RMAX = DRAIN ? 64 : 1;
+    float R[RMAX];
+    long u = 0;
+    bool ok = true;
+    for (long t = blockIdx.x; ok && t < p.num_tiles; t += gridDim.x) {
+      const TileInfo ti = decode_tile(p, t);
+      int gi, i, jlo, jhi;
+      bool rok;
+      if (p.G > 1) {
+        gi = r / p.M; i = r - gi * p.M; rok = gi < ti.ng;
+        jlo = gi * p.N; jhi = jlo + p.N;
+      } else {
+        gi = 0; i = ti.m0 + r; rok = i < p.M;
+        jlo = 0; jhi = min(tn, p.N - ti.n0);
+      }
+      float *crow = p.C + (ti.g0 + gi) * p.sC + (long)i * p.ldc + (ti.n0 - jlo);
+      const bool vec = p.vec_c && ((p.G == 1) || (p.N % 4 == 0));
+      auto store8 = [&](int ch, const float *v) {
+        const int j0 = ch * 8;
+        if (!rok || j0 + 8 <= jlo || j0 >= jhi) return;
+        if (vec && j0 >= jlo && j0 + 8 <= jhi) {
+          float4 o0, o1;
+          if (p.beta != 0.0f) {
+            const float4 c0 = *reinterpret_cast<const float4 *>(crow + j0);
+            const float4 c1 = *reinterpret_cast<const float4 *>(crow + j0 + 4);
+            o0 = make_float4(__fmaf_rn(p.beta, c0.x, p.alpha * v[0]),
+                             __fmaf_rn(p.beta, c0.y, p.alpha * v[1]),
+                             __fmaf_rn(p.beta, c0.z, p.alpha * v[2]),
+                             __fmaf_rn(p.beta, c0.w, p.alpha * v[3]));
+            o1 = make_float4(__fmaf_rn(p.beta, c1.x, p.alpha * v[4]),
+                             __fmaf_rn(p.beta, c1.y, p.alpha * v[5]),
+                             __fmaf_rn(p.beta, c1.z, p.alpha * v[6]),
+                             __fmaf_rn(p.beta, c1.w, p.alpha * v[7]));
+          } else {
+            o0 = make_float4(p.alpha * v[0], p.alpha * v[1], p.alpha * v[2], p.alpha * v[3]);
+            o1 = make_float4(p.alpha * v[4], p.alpha * v[5], p.alpha * v[6], p.alpha * v[7]);
+          }
+          *reinterpret_cast<float4 *>(crow + j0) = o0;
+          *reinterpret_cast<float4 *>(crow + j0 + 4) = o1;
+        } else {
+#pragma unroll
+          for (int w = 0; w < 8; ++w) {
+            const int jc = j0 + w;
+            if (jc >= jlo && jc < jhi) {
+              float x = p.alpha * v[w];
+              if (p.beta != 0.0f) x = __fmaf_rn(p.beta, crow[jc], x);
+              crow[jc] = x;
+            }
+          }
+        }
+      };
+      const int nchunks = DRAIN ? (p.nk + kc - 1) / kc : 1;
+#pragma unroll
+      for (int w = 0; w < RMAX; ++w) R[w] = 0.0f;
+      for (int cu = 0; cu < nchunks; ++cu, ++u) {
+        const int a = (int)(u & 1);
+        if (!ws_wait(&bars[B_AFULL + a], (uint32_t)((u >> 1) & 1), s_abort, p.err)) {
+          ok = false;
+          break;
+        }
+        ptx::tc_fence_after();
+        const uint32_t acc_base = tmem + ((uint32_t)(wq * 32) << 16) + (uint32_t)(a * 256);
+        if constexpr (DRAIN) {
+#pragma unroll
+          for (int q = 0; q < 8; ++q) {
+            const int ch = c_begin + q;
+            if (ch < c_end) {
+              float dm[8], dc[8];
+              ptx::tmem_ld8(acc_base + ch * 8, dm);
+              ptx::tmem_ld8(acc_base + 128 + ch * 8, dc);
+              ptx::tmem_wait_ld();
+#pragma unroll
+              for (int w = 0; w < 8; ++w) R[q * 8 + w] += dm[w] + dc[w];
+            }
+          }
+          ptx::tc_fence_before();
+          __syncwarp();
+          if (lane == 0) mbar_arrive(&bars[B_AEMPTY + a]);
+        } else {
+          for (int ch = c_begin; ch < c_end; ++ch) {
+            float dm[8], dc[8];
+            ptx::tmem_ld8(acc_base + ch * 8, dm);
+            ptx::tmem_ld8(acc_base + 128 + ch * 8, dc);
+            ptx::tmem_wait_ld();
+#pragma unroll
+            for (int w = 0; w < 8; ++w) dm[w] += dc[w];
+            store8(ch, dm);
+          }
+          ptx::tc_fence_before();
+          __syncwarp();
+          if (lane == 0) mbar_arrive(&bars[B_AEMPTY + a]);
+        }
+      }
+      if constexpr (DRAIN) {
+        if (ok) {
+#pragma unroll
+          for (int q = 0; q < 8; ++q) {
+            const int ch = c_begin + q;
+            if (ch < c_end) store8(ch, R + q * 8);
+          }
+        }
+      }
+    }
+  }
+
+  __syncthreads();
+  if (warp == 1) {
+    ptx::tc_fence_after();
+    ptx::tmem_dealloc(tmem, WS_TMEM_COLS);
+  }
+}
+
 // device status word for the bounded waits
 __device__ unsigned g_tc_err;
+
+// cuTensorMapEncodeTiled through the runtime's driver entry point (the
+// library does not link libcuda directly)
+PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  static bool tried = false;
+  if (!tried) {
+    tried = true;
+    void *f = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &q) ==
+            cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(f);
+    else
+      cudaGetLastError();
+  }
+  return fn;
+}
+
+bool aligned16(const void *ptr) { return (reinterpret_cast<uintptr_t>(ptr) & 15) == 0; }
+
+// 3-D FP32 tensor map: dims (d0 innermost, d1, d2), byte strides of d1 and d2.
+bool encode_map(CUtensorMap *map, const float *base, uint64_t d0, uint64_t d1, uint64_t d2,
+                uint64_t s1_bytes, uint64_t s2_bytes, uint32_t b0, uint32_t b1, uint32_t b2,
+                bool swizzle128) {
+  PFN_cuTensorMapEncodeTiled_v12000 enc = tensor_map_encoder();
+  if (!enc) return false;
+  const cuuint64_t dims[3] = {d0, d1, d2};
+  const cuuint64_t strides[2] = {s1_bytes, s2_bytes};
+  const cuuint32_t box[3] = {b0, b1, b2};
+  const cuuint32_t estr[3] = {1, 1, 1};
+  const CUresult r = enc(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, const_cast<float *>(base), dims,
+                         strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                         swizzle128 ? CU_TENSOR_MAP_SWIZZLE_128B : CU_TENSOR_MAP_SWIZZLE_NONE,
+                         CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS;
+}
+
+// Tensor maps for the warp-specialized kernel, or false when TMA cannot
+// address the operands (unaligned base or row stride, overlapping batches).
+bool ws_maps(const TcProblem &p, CUtensorMap *ma, CUtensorMap *mb, WsArgs *wa) {
+  const long count = p.count;
+  const long sA = count > 1 ? p.sA : (long)p.M * p.lda;
+  const long rowsB = p.transb ? p.N : p.K;
+  const long sB = count > 1 ? p.sB : rowsB * p.ldb;
+  if (!aligned16(p.A) || !aligned16(p.B) || p.lda % 4 || p.ldb % 4 || sA % 4 || sB % 4)
+    return false;
+  if (count > 1 && (sA < (long)p.M * p.lda || sB < rowsB * p.ldb)) return false;
+  const bool packed = p.G > 1;
+  if (packed && !p.transb && p.N % 4) return false;  // B box rows must be 16-byte multiples
+  const uint32_t a1 = packed ? p.M : TC_BM, a2 = packed ? p.G : 1;
+  if (!encode_map(ma, p.A, p.K, p.M, count, (uint64_t)p.lda * 4, (uint64_t)sA * 4, TC_BK, a1,
+                  a2, true))
+    return false;
+  uint32_t b0, b1, b2;
+  if (p.transb) {
+    b0 = TC_BK; b1 = packed ? p.N : p.tile_n; b2 = packed ? p.G : 1;
+    if (!encode_map(mb, p.B, p.K, p.N, count, (uint64_t)p.ldb * 4, (uint64_t)sB * 4, b0, b1, b2,
+                    true))
+      return false;
+  } else {
+    b0 = packed ? p.N : p.tile_n; b1 = TC_BK; b2 = packed ? p.G : 1;
+    if (!encode_map(mb, p.B, p.N, p.K, count, (uint64_t)p.ldb * 4, (uint64_t)sB * 4, b0, b1, b2,
+                    false))
+      return false;
+  }
+  wa->p = p;
+  wa->tx_bytes = (uint32_t)(TC_BK * a1 * a2 + b0 * b1 * b2) * 4;
+  wa->nn_w = p.transb ? 0 : (int)b0;
+  return true;
+}
 
 int tc_launch(TcProblem &p, int mode) {
   State &st = state();
@@ -554,13 +1007,25 @@ int tc_launch(TcProblem &p, int mode) {
   LS_CUDA_TRY(cudaGetSymbolAddress(&errp, g_tc_err));
   p.err = reinterpret_cast<unsigned *>(errp);
   const bool drain = p.nk > p.kc_slabs;
-  const void *kern = mode == LIBSHALOM_PREC_BF16X6
-                         ? (drain ? (const void *)k_tc_sgemm<3, true> : (const void *)k_tc_sgemm<3, false>)
-                         : (drain ? (const void *)k_tc_sgemm<2, true> : (const void *)k_tc_sgemm<2, false>);
-  (void)occupancy_of(kern, TC_THREADS, TC_SMEM, 1);  // raises the shared-memory limit
-  const int grid = grid_for(p.num_tiles, 1);
-  void *args[] = {&p};
-  LS_CUDA_TRY(cudaLaunchKernel(kern, dim3(grid), dim3(TC_THREADS), args, TC_SMEM, st.stream));
+  CUtensorMap ma, mb;
+  WsArgs wa;
+  if (st.use_tma && ws_maps(p, &ma, &mb, &wa)) {
+    const void *kern = mode == LIBSHALOM_PREC_BF16X6
+                           ? (drain ? (const void *)k_tc_ws<3, true> : (const void *)k_tc_ws<3, false>)
+                           : (drain ? (const void *)k_tc_ws<2, true> : (const void *)k_tc_ws<2, false>);
+    (void)occupancy_of(kern, WS_THREADS, WS_SMEM, 1);  // raises the shared-memory limit
+    const int grid = grid_for(p.num_tiles, 1);
+    void *args[] = {&ma, &mb, &wa};
+    LS_CUDA_TRY(cudaLaunchKernel(kern, dim3(grid), dim3(WS_THREADS), args, WS_SMEM, st.stream));
+  } else {
+    const void *kern = mode == LIBSHALOM_PREC_BF16X6
+                           ? (drain ? (const void *)k_tc_sgemm<3, true> : (const void *)k_tc_sgemm<3, false>)
+                           : (drain ? (const void *)k_tc_sgemm<2, true> : (const void *)k_tc_sgemm<2, false>);
+    (void)occupancy_of(kern, TC_THREADS, TC_SMEM, 1);  // raises the shared-memory limit
+    const int grid = grid_for(p.num_tiles, 1);
+    void *args[] = {&p};
+    LS_CUDA_TRY(cudaLaunchKernel(kern, dim3(grid), dim3(TC_THREADS), args, TC_SMEM, st.stream));
+  }
   LS_CUDA_TRY(cudaGetLastError());
   if (st.sync) {
     // synchronous mode: report an expired device-side wait as a status
@@ -575,8 +1040,6 @@ int tc_launch(TcProblem &p, int mode) {
   }
   return LIBSHALOM_SUCCESS;
 }
-
-bool aligned16(const void *ptr) { return (reinterpret_cast<uintptr_t>(ptr) & 15) == 0; }
 
 void plan_tiles(TcProblem &p) {
   if (p.M <= 64 && p.N <= 64) {

@@ -21,6 +21,15 @@ TOL = {ls.PREC_BF16X6: (1e-6, 8 * 2.0 ** -24), ls.PREC_BF16X3: (2e-5, 2.0 ** -14
 def mode_setter():
     yield ls.set_precision
     ls.set_precision(ls.PREC_FP32)
+    ls.set_tma(True)
+
+
+@pytest.fixture(params=[True, False], ids=["tma", "cpasync"])
+def staging(request):
+    """both operand-staging variants of the tensor-core kernel"""
+    ls.set_tma(request.param)
+    yield request.param
+    ls.set_tma(True)
 
 
 def _strided(mode, transb, M, N, K, count, seed, alpha=1.0, beta=0.0):
@@ -50,7 +59,7 @@ def _check(C, A, B, transb, mode, alpha=1.0, beta=0.0, C0=None):
 @pytest.mark.parametrize("mode", [ls.PREC_BF16X6, ls.PREC_BF16X3])
 @pytest.mark.parametrize("transb", [0, 1])
 @pytest.mark.parametrize("n", list(range(8, 129, 8)))
-def test_tc_cube_sweep(n, transb, mode, mode_setter):
+def test_tc_cube_sweep(n, transb, mode, mode_setter, staging):
     count = 37
     A, B, _, C = _strided(mode, transb, n, n, n, count, seed=100 + n + 7 * transb)
     for g in (0, 1, count // 2, count - 1):
@@ -61,7 +70,7 @@ def test_tc_cube_sweep(n, transb, mode, mode_setter):
 @pytest.mark.parametrize("M,N,K", [(1, 1, 1), (3, 5, 7), (13, 9, 33), (17, 31, 15),
                                    (64, 64, 64), (65, 17, 40), (100, 130, 70),
                                    (129, 7, 200), (33, 129, 31), (200, 250, 257)])
-def test_tc_ragged(M, N, K, transb, mode_setter):
+def test_tc_ragged(M, N, K, transb, mode_setter, staging):
     count = 9
     A, B, _, C = _strided(ls.PREC_BF16X6, transb, M, N, K, count, seed=M * 7 + N * 3 + K)
     for g in range(count):
@@ -76,7 +85,7 @@ def test_tc_alpha_beta(mode_setter):
 
 @pytest.mark.parametrize("M,N,K", [(64, 392, 576), (128, 98, 1152), (512, 49, 960),
                                    (2048, 32, 2560), (32, 2048, 1024)])
-def test_tc_sgemm_mp(M, N, K, mode_setter):
+def test_tc_sgemm_mp(M, N, K, mode_setter, staging):
     import torch
     A, B = orc.gemm_inputs_f32(M + 2 * N + K, M, N, K, 0)
     dC = torch.full((M, N), float("nan"), device="cuda")
@@ -85,7 +94,7 @@ def test_tc_sgemm_mp(M, N, K, mode_setter):
     _check(to_host(dC), A, B, 0, ls.PREC_BF16X6)
 
 
-def test_tc_large_batch_spot_check(mode_setter):
+def test_tc_large_batch_spot_check(mode_setter, staging):
     # many tiles per CTA: the persistent loop, buffer/phase reuse across tiles
     count, n = 3000, 40
     A, B, _, C = _strided(ls.PREC_BF16X6, 0, n, n, n, count, seed=9)
