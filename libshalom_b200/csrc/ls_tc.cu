@@ -782,15 +782,19 @@ __global__ void __launch_bounds__(WS_THREADS, 1)
               x[4] = u1.x; x[5] = u1.y; x[6] = u1.z; x[7] = u1.w;
             } else {
               // [g][32 k][nn_w] (packed) or [32 k][tn]: column jj of GEMM g = jj / N
+              // padding columns past the G packed GEMMs are not in the box: zero
               const float *fb = reinterpret_cast<const float *>(stg + 16384);
               int col = jj, gofs = 0;
+              bool in_box = true;
               if (p.G > 1) {
                 const int g = jj / p.N;
                 col = jj - g * p.N;
                 gofs = g * 32 * nn_w;
+                in_box = g < p.G;
               }
 #pragma unroll
-              for (int tk = 0; tk < 8; ++tk) x[tk] = fb[gofs + (8 * c + tk) * nn_w + col];
+              for (int tk = 0; tk < 8; ++tk)
+                x[tk] = in_box ? fb[gofs + (8 * c + tk) * nn_w + col] : 0.0f;
             }
             uint4 h, m, l;
             split8<NSPLIT>(x, h, m, l);
