@@ -52,12 +52,16 @@ def step_bytes(batch=BATCH):
 def parse():
     p = argparse.ArgumentParser()
     p.add_argument("--gpus", type=int, default=1)
-    p.add_argument("--steps", type=int, default=20)
+    p.add_argument("--steps", type=int, default=50)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="b200", choices=["b200", "reference"])
     p.add_argument("--mode", default="auto", choices=["auto", "fp32", "bf16x3", "bf16x6"])
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu", action="store_true")
+    # smaller cases of the same workload, for profiling (not the bench line)
+    p.add_argument("--sizes", default=None, help="comma list of cube sizes (default 8..128)")
+    p.add_argument("--batch", type=int, default=None, help="GEMMs per size (default 10000)")
+    p.add_argument("--layouts", default=None, help="nn, nt or nn,nt (default both)")
     return p.parse_args()
 
 
@@ -308,6 +312,7 @@ def run_gpu(args):
     # final timed run of the headline mode with clocks sampled
     clocks = Clocks(local)
     clocks.start()
+    time.sleep(0.5)  # nvidia-smi needs a moment before its first sample
     total_ms, kern_ms = timed(best)
     clk = clocks.stop()
     ms_step = total_ms / args.steps
@@ -415,7 +420,14 @@ def run_gpu(args):
 
 
 def main():
+    global SIZES, BATCH, LAYOUTS
     args = parse()
+    if args.sizes:
+        SIZES = [int(x) for x in args.sizes.split(",")]
+    if args.batch:
+        BATCH = args.batch
+    if args.layouts:
+        LAYOUTS = tuple({"nn": 0, "nt": 1}[x] for x in args.layouts.split(","))
     if args.impl == "reference":
         return run_reference(args)
     return run_gpu(args)

@@ -930,6 +930,544 @@ __global__ void __launch_bounds__(WS_THREADS, 1)
   }
 }
 
+// ===========================================================================
+// Grouped batches (LibShalom_sgemm_batched): arbitrary per-GEMM pointers,
+// shapes, transposes, leading dimensions, alpha and beta, read from device
+// entries.  Same converter / MMA / epilogue warps as the TMA kernel; the
+// producer is two warps of cp.async (any alignment) whose completion arrives
+// on the stage's mbarrier (cp.async.mbarrier.arrive.noinc).  The FP32 slab is
+// staged in the same layout the TMA kernel uses (A and B (Trans) rows of 128
+// bytes with the 128-byte swizzle, B (NoTrans) as [32 k][tile_n]).
+//
+// Work plan (built on the device, sized by the entry count alone, so a call
+// needs no host round trip): runs of entries sharing C are sorted by their K
+// work (counting sort over GRP_CLASSES classes, heaviest first) and a prefix
+// sum of their tile counts maps a global tile index to (run, 128-row tile,
+// N tile) by binary search.  Static round-robin over that heaviest-first order
+// balances the persistent CTAs.  The products of a run are applied in array
+// order by the one CTA that owns the tile (C = alpha_p A_p op(B_p) + beta_p C,
+// product by product).
+// ===========================================================================
+struct GrpItem {
+  int first;  // first entry of the run
+  int len;    // entries in the run
+  int m0, n0;
+};
+
+constexpr int GRP_CLASSES = 64;  // work classes (total K slabs of the run, capped)
+
+// workspace layout of the plan (unsigned words)
+struct GrpPlan {
+  unsigned *class_runs;   // [GRP_CLASSES] runs per class
+  unsigned *class_off;    // [GRP_CLASSES] first sorted slot of each class
+  unsigned *class_fill;   // [GRP_CLASSES] slots taken so far
+  unsigned *n_runs;       // [1]
+  unsigned *run_first;    // [count] first entry of the run in sorted slot s
+  unsigned *run_len;      // [count]
+  unsigned *tile_prefix;  // [count + 1] exclusive prefix of tiles over sorted slots
+};
+
+struct GrpArgs {
+  const LibShalom_sgemm_entry *entries;
+  long count;
+  const unsigned *run_first, *run_len, *tile_prefix, *n_runs;
+  unsigned *err;
+  int kc_slabs;
+};
+
+constexpr int G_PROD_WARPS = 2, G_W_MMA = 2, G_W_CONV0 = 3, G_W_EPI0 = 11;
+constexpr int G_WARPS = 19;
+constexpr int G_THREADS = G_WARPS * 32;
+
+__device__ __forceinline__ int grp_tile_n(int N) { return min(TC_MAX_N, (N + 15) / 16 * 16); }
+
+__device__ __forceinline__ bool grp_run_start(const LibShalom_sgemm_entry *e, long i) {
+  return i == 0 || e[i].C != e[i - 1].C;
+}
+
+// K work of the run starting at entry i (capped class index) and its length
+__device__ __forceinline__ int grp_run_class(const LibShalom_sgemm_entry *e, long count, long i,
+                                             long *len) {
+  long slabs = 0, j = i;
+  do {
+    slabs += max(1, (e[j].K + TC_BK - 1) / TC_BK);
+    ++j;
+  } while (j < count && e[j].C == e[i].C);
+  *len = j - i;
+  return (int)min(slabs, (long)GRP_CLASSES - 1);
+}
+
+__device__ __forceinline__ unsigned grp_run_tiles(const LibShalom_sgemm_entry &e) {
+  if (e.M <= 0 || e.N <= 0) return 0;
+  const int tn = grp_tile_n(e.N);
+  return (unsigned)(((e.M + TC_BM - 1) / TC_BM) * ((e.N + tn - 1) / tn));
+}
+
+// pass 1: runs per work class
+__global__ void k_grp_count(const LibShalom_sgemm_entry *e, long count, GrpPlan pl) {
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < count;
+       i += (long)gridDim.x * blockDim.x) {
+    if (!grp_run_start(e, i)) continue;
+    long len;
+    atomicAdd(&pl.class_runs[grp_run_class(e, count, i, &len)], 1u);
+  }
+}
+
+// pass 2: first sorted slot of every class, heaviest class first
+__global__ void k_grp_offsets(GrpPlan pl) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) {
+    unsigned acc = 0;
+    for (int c = GRP_CLASSES - 1; c >= 0; --c) {
+      pl.class_off[c] = acc;
+      acc += pl.class_runs[c];
+    }
+    *pl.n_runs = acc;
+  }
+}
+
+// pass 3: every run takes a slot in its class's range
+__global__ void k_grp_place(const LibShalom_sgemm_entry *e, long count, GrpPlan pl) {
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < count;
+       i += (long)gridDim.x * blockDim.x) {
+    if (!grp_run_start(e, i)) continue;
+    long len;
+    const int cls = grp_run_class(e, count, i, &len);
+    const unsigned slot = pl.class_off[cls] + atomicAdd(&pl.class_fill[cls], 1u);
+    pl.run_first[slot] = (unsigned)i;
+    pl.run_len[slot] = (unsigned)len;
+  }
+}
+
+// pass 4 (one CTA of 1024 threads): exclusive prefix of tiles over the slots
+__global__ void __launch_bounds__(1024) k_grp_prefix(const LibShalom_sgemm_entry *e, GrpPlan pl) {
+  __shared__ unsigned warp_sums[32];
+  __shared__ unsigned carry;
+  const unsigned R = *pl.n_runs;
+  if (threadIdx.x == 0) carry = 0;
+  __syncthreads();
+  for (unsigned base = 0; base < R; base += 1024) {
+    const unsigned s = base + threadIdx.x;
+    const unsigned v = s < R ? grp_run_tiles(e[pl.run_first[s]]) : 0u;
+    unsigned x = v;  // inclusive warp scan
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const unsigned y = __shfl_up_sync(0xffffffffu, x, o);
+      if ((threadIdx.x & 31) >= (unsigned)o) x += y;
+    }
+    if ((threadIdx.x & 31) == 31) warp_sums[threadIdx.x >> 5] = x;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+      unsigned w = warp_sums[threadIdx.x];
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const unsigned y = __shfl_up_sync(0xffffffffu, w, o);
+        if (threadIdx.x >= (unsigned)o) w += y;
+      }
+      warp_sums[threadIdx.x] = w;  // inclusive over warps
+    }
+    __syncthreads();
+    const unsigned warp_off = (threadIdx.x >> 5) ? warp_sums[(threadIdx.x >> 5) - 1] : 0u;
+    if (s < R) pl.tile_prefix[s] = carry + warp_off + x - v;
+    __syncthreads();
+    if (threadIdx.x == 0) carry += warp_sums[31];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) pl.tile_prefix[R] = carry;
+}
+
+// global tile index -> (run, 128-row tile, N tile)
+__device__ __forceinline__ GrpItem grp_item(const GrpArgs &g, long t) {
+  int lo = 0, hi = (int)*g.n_runs - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if ((long)g.tile_prefix[mid] <= t) lo = mid;
+    else hi = mid - 1;
+  }
+  GrpItem it;
+  it.first = (int)g.run_first[lo];
+  it.len = (int)g.run_len[lo];
+  const int local = (int)(t - (long)g.tile_prefix[lo]);
+  const int N = g.entries[it.first].N;
+  const int tn = grp_tile_n(N);
+  const int tn_n = (N + tn - 1) / tn;
+  it.m0 = (local / tn_n) * TC_BM;
+  it.n0 = (local % tn_n) * tn;
+  return it;
+}
+
+// one product of a work item, as every role sees it
+struct GrpJob {
+  const float *A, *B;
+  float *C;
+  int M, N, K, lda, ldb, ldc, transb, nk, tn;
+  float alpha, beta;
+  bool vec_a, vec_b;
+};
+
+__device__ __forceinline__ GrpJob grp_job(const GrpArgs &g, const GrpItem &it, int p) {
+  const LibShalom_sgemm_entry &e = g.entries[it.first + p];
+  GrpJob j;
+  j.A = e.A; j.B = e.B; j.C = e.C;
+  j.M = e.M; j.N = e.N; j.K = max(0, e.K);
+  j.transb = e.transb;
+  j.lda = e.lda > 0 ? e.lda : j.K;
+  j.ldb = e.ldb > 0 ? e.ldb : (e.transb ? j.K : j.N);
+  j.ldc = e.ldc > 0 ? e.ldc : j.N;
+  j.alpha = e.alpha; j.beta = e.beta;
+  j.nk = max(1, (j.K + TC_BK - 1) / TC_BK);
+  j.tn = grp_tile_n(j.N);
+  j.vec_a = (reinterpret_cast<uintptr_t>(j.A) & 15) == 0 && (j.lda & 3) == 0;
+  j.vec_b = (reinterpret_cast<uintptr_t>(j.B) & 15) == 0 && (j.ldb & 3) == 0;
+  return j;
+}
+
+__device__ __forceinline__ void cp_async_mbar_arrive(uint64_t *bar) {
+  asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];" ::"r"(ptx::smem_u32(bar))
+               : "memory");
+}
+
+template <int NSPLIT>
+__global__ void __launch_bounds__(G_THREADS, 1) k_tc_grouped(const GrpArgs g) {
+  extern __shared__ __align__(1024) unsigned char smem[];
+  uint64_t *bars = reinterpret_cast<uint64_t *>(smem + WS_OFF_BAR);
+  uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(smem + WS_OFF_BAR + 8 * B_COUNT);
+  volatile int *s_abort = reinterpret_cast<volatile int *>(smem + WS_OFF_BAR + 8 * B_COUNT + 4);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const uint32_t smem_base = ptx::smem_u32(smem);
+  const int kc = g.kc_slabs;
+  const long n_items = (long)g.tile_prefix[*g.n_runs];
+
+  if (tid == 0) {
+    for (int i = 0; i < WS_STAGES; ++i) {
+      ptx::mbar_init(&bars[B_FULL + i], G_PROD_WARPS * 32);
+      ptx::mbar_init(&bars[B_EMPTY + i], N_CONV);
+    }
+    for (int i = 0; i < 2; ++i) {
+      ptx::mbar_init(&bars[B_BFULL + i], N_CONV);
+      ptx::mbar_init(&bars[B_BEMPTY + i], 1);
+      ptx::mbar_init(&bars[B_AFULL + i], 1);
+      ptx::mbar_init(&bars[B_AEMPTY + i], N_EPI);
+    }
+    ptx::mbar_init(&bars[B_FINAL], 1);
+    *s_abort = 0;
+    ptx::fence_mbar_init();
+  }
+  if (warp == G_W_MMA) {
+    ptx::tmem_alloc(tmem_slot, WS_TMEM_COLS);
+    ptx::tmem_relinquish();
+  }
+  ptx::tc_fence_before();
+  __syncthreads();
+  ptx::tc_fence_after();
+  const uint32_t tmem = *tmem_slot;
+
+  if (warp < G_PROD_WARPS) {
+    // ------------------------- producer (cp.async) -------------------------
+    const int pt = tid;  // 0..63
+    long j = 0;
+    bool ok = true;
+    for (long t = blockIdx.x; ok && t < n_items; t += gridDim.x) {
+      const GrpItem it = grp_item(g, t);
+      for (int pidx = 0; ok && pidx < it.len; ++pidx) {
+        const GrpJob jb = grp_job(g, it, pidx);
+        for (int s = 0; s < jb.nk; ++s, ++j) {
+          const int st = (int)(j % WS_STAGES);
+          if (j >= WS_STAGES &&
+              !ws_wait(&bars[B_EMPTY + st], (uint32_t)(((j / WS_STAGES) - 1) & 1), s_abort, g.err)) {
+            ok = false;
+            break;
+          }
+          const uint32_t sa = smem_base + WS_OFF_STAGE + st * WS_STAGE_BYTES;
+          const uint32_t sb = sa + 16384;
+          const int k0 = s * TC_BK;
+          // A: 128 rows x 8 chunks of 4 floats; swizzled 128-byte rows
+          for (int e = pt; e < 128 * 8; e += G_PROD_WARPS * 32) {
+            const int r = e >> 3, q = e & 7;
+            const int row = it.m0 + r, k = k0 + 4 * q;
+            const uint32_t dst = sa + r * 128 + ((q ^ (r & 7)) << 4);
+            const float *src = jb.A + (long)row * jb.lda + k;
+            if (jb.vec_a) {
+              const int n = (row < jb.M && k < jb.K) ? 4 * min(4, jb.K - k) : 0;
+              cp_async16(dst, n ? src : jb.A, n);
+            } else {
+#pragma unroll
+              for (int w = 0; w < 4; ++w) {
+                const bool v = row < jb.M && k + w < jb.K;
+                cp_async4(dst + 4 * w, v ? src + w : jb.A, v ? 4 : 0);
+              }
+            }
+          }
+          if (jb.transb) {
+            for (int e = pt; e < jb.tn * 8; e += G_PROD_WARPS * 32) {
+              const int r = e >> 3, q = e & 7;
+              const int row = it.n0 + r, k = k0 + 4 * q;
+              const uint32_t dst = sb + r * 128 + ((q ^ (r & 7)) << 4);
+              const float *src = jb.B + (long)row * jb.ldb + k;
+              if (jb.vec_b) {
+                const int n = (row < jb.N && k < jb.K) ? 4 * min(4, jb.K - k) : 0;
+                cp_async16(dst, n ? src : jb.B, n);
+              } else {
+#pragma unroll
+                for (int w = 0; w < 4; ++w) {
+                  const bool v = row < jb.N && k + w < jb.K;
+                  cp_async4(dst + 4 * w, v ? src + w : jb.B, v ? 4 : 0);
+                }
+              }
+            }
+          } else {
+            const int cpr = jb.tn >> 2;
+            for (int e = pt; e < 32 * cpr; e += G_PROD_WARPS * 32) {
+              const int kr = e / cpr, col = (e - kr * cpr) * 4;
+              const int k = k0 + kr, n = it.n0 + col;
+              const uint32_t dst = sb + (kr * jb.tn + col) * 4;
+              const float *src = jb.B + (long)k * jb.ldb + n;
+              if (jb.vec_b) {
+                const int nb = (k < jb.K && n < jb.N) ? 4 * min(4, jb.N - n) : 0;
+                cp_async16(dst, nb ? src : jb.B, nb);
+              } else {
+#pragma unroll
+                for (int w = 0; w < 4; ++w) {
+                  const bool v = k < jb.K && n + w < jb.N;
+                  cp_async4(dst + 4 * w, v ? src + w : jb.B, v ? 4 : 0);
+                }
+              }
+            }
+          }
+          cp_async_mbar_arrive(&bars[B_FULL + st]);  // arrives when this thread's copies land
+        }
+      }
+    }
+    cp_async_wait<0>();
+  } else if (warp == G_W_MMA) {
+    // -------------------------------- MMA ---------------------------------
+    if (lane == 0) {
+      long j = 0, u = 0;
+      bool ok = true;
+      for (long t = blockIdx.x; ok && t < n_items; t += gridDim.x) {
+        const GrpItem it = grp_item(g, t);
+        for (int pidx = 0; ok && pidx < it.len; ++pidx) {
+          const GrpJob jb = grp_job(g, it, pidx);
+          const uint32_t idesc = ptx::idesc_bf16_f32(TC_BM, jb.tn);
+          for (int s = 0; s < jb.nk; ++s, ++j) {
+            const int s_in = s % kc;
+            if (s_in == 0) {
+              const int a = (int)(u & 1);
+              if (u >= 2 && !ws_wait(&bars[B_AEMPTY + a], (uint32_t)(((u >> 1) - 1) & 1), s_abort,
+                                     g.err)) {
+                ok = false;
+                break;
+              }
+            }
+            const int b = (int)(j & 1);
+            if (!ws_wait(&bars[B_BFULL + b], (uint32_t)((j >> 1) & 1), s_abort, g.err)) {
+              ok = false;
+              break;
+            }
+            ptx::tc_fence_after();
+            const uint32_t acc_base = tmem + (uint32_t)((u & 1) * 256);
+            const uint32_t bb = smem_base + WS_OFF_BUF + b * BUF_BYTES;
+            const int ksteps = max(1, min(2, (jb.K - s * TC_BK + 15) / 16));
+#pragma unroll
+            for (int ks = 0; ks < 2; ++ks) {
+              if (ks >= ksteps) break;
+              const uint32_t acc = (s_in > 0 || ks > 0) ? 1u : 0u;
+              uint64_t da[3], db[3];
+#pragma unroll
+              for (int sp = 0; sp < NSPLIT; ++sp) {
+                da[sp] = ptx::smem_desc(bb + sp * SPLIT_BYTES + ks * 2 * CHUNK_BYTES, CHUNK_BYTES, 128);
+                db[sp] = ptx::smem_desc(bb + sp * SPLIT_BYTES + 8192 + ks * 2 * CHUNK_BYTES,
+                                        CHUNK_BYTES, 128);
+              }
+              ptx::mma_bf16(acc_base, da[0], db[0], idesc, acc);
+              ptx::mma_bf16(acc_base + 128, da[0], db[1], idesc, acc);
+              ptx::mma_bf16(acc_base + 128, da[1], db[0], idesc, 1u);
+              if (NSPLIT == 3) {
+                ptx::mma_bf16(acc_base + 128, da[0], db[2], idesc, 1u);
+                ptx::mma_bf16(acc_base + 128, da[2], db[0], idesc, 1u);
+                ptx::mma_bf16(acc_base + 128, da[1], db[1], idesc, 1u);
+              }
+            }
+            ptx::mma_commit(&bars[B_BEMPTY + b]);
+            if (s_in == kc - 1 || s == jb.nk - 1) {
+              ptx::mma_commit(&bars[B_AFULL + (u & 1)]);
+              ++u;
+            }
+          }
+        }
+      }
+      ptx::mma_commit(&bars[B_FINAL]);
+      ptx::mbar_wait_bounded(&bars[B_FINAL], 0);
+    }
+  } else if (warp < G_W_EPI0) {
+    // ----------------------------- converters -----------------------------
+    const int ct = tid - G_W_CONV0 * 32;
+    const int cr = ct & 127, cc0 = ct >> 7;
+    long j = 0;
+    bool ok = true;
+    for (long t = blockIdx.x; ok && t < n_items; t += gridDim.x) {
+      const GrpItem it = grp_item(g, t);
+      for (int pidx = 0; ok && pidx < it.len; ++pidx) {
+        const GrpJob jb = grp_job(g, it, pidx);
+        const int tn = jb.tn;
+        for (int s = 0; s < jb.nk; ++s, ++j) {
+          const int st = (int)(j % WS_STAGES), b = (int)(j & 1);
+          if (!ws_wait(&bars[B_FULL + st], (uint32_t)((j / WS_STAGES) & 1), s_abort, g.err)) {
+            ok = false;
+            break;
+          }
+          if (j >= 2 && !ws_wait(&bars[B_BEMPTY + b], (uint32_t)(((j >> 1) - 1) & 1), s_abort,
+                                 g.err)) {
+            ok = false;
+            break;
+          }
+          const unsigned char *stg = smem + WS_OFF_STAGE + st * WS_STAGE_BYTES;
+          unsigned char *base = smem + WS_OFF_BUF + b * BUF_BYTES;
+#pragma unroll
+          for (int q = 0; q < 2; ++q) {
+            const int c = cc0 + 2 * q;
+            const unsigned char *row = stg + cr * 128;
+            const float4 u0 = *reinterpret_cast<const float4 *>(row + (((2 * c) ^ (cr & 7)) << 4));
+            const float4 u1 =
+                *reinterpret_cast<const float4 *>(row + (((2 * c + 1) ^ (cr & 7)) << 4));
+            float x[8] = {u0.x, u0.y, u0.z, u0.w, u1.x, u1.y, u1.z, u1.w};
+            uint4 h, m, l;
+            split8<NSPLIT>(x, h, m, l);
+            const int off = c * CHUNK_BYTES + cr * 16;
+            *reinterpret_cast<uint4 *>(base + off) = h;
+            *reinterpret_cast<uint4 *>(base + SPLIT_BYTES + off) = m;
+            if (NSPLIT == 3) *reinterpret_cast<uint4 *>(base + 2 * SPLIT_BYTES + off) = l;
+          }
+#pragma unroll
+          for (int q = 0; q < 2; ++q) {
+            const int e = ct + q * 256;
+            if (e < 4 * tn) {
+              const int jj = e % tn, c = e / tn;
+              float x[8];
+              if (jb.transb) {
+                const unsigned char *row = stg + 16384 + jj * 128;
+                const float4 u0 =
+                    *reinterpret_cast<const float4 *>(row + (((2 * c) ^ (jj & 7)) << 4));
+                const float4 u1 =
+                    *reinterpret_cast<const float4 *>(row + (((2 * c + 1) ^ (jj & 7)) << 4));
+                x[0] = u0.x; x[1] = u0.y; x[2] = u0.z; x[3] = u0.w;
+                x[4] = u1.x; x[5] = u1.y; x[6] = u1.z; x[7] = u1.w;
+              } else {
+                const float *fb = reinterpret_cast<const float *>(stg + 16384);
+#pragma unroll
+                for (int tk = 0; tk < 8; ++tk) x[tk] = fb[(8 * c + tk) * tn + jj];
+              }
+              uint4 h, m, l;
+              split8<NSPLIT>(x, h, m, l);
+              const int off = 8192 + c * CHUNK_BYTES + jj * 16;
+              *reinterpret_cast<uint4 *>(base + off) = h;
+              *reinterpret_cast<uint4 *>(base + SPLIT_BYTES + off) = m;
+              if (NSPLIT == 3) *reinterpret_cast<uint4 *>(base + 2 * SPLIT_BYTES + off) = l;
+            }
+          }
+          ptx::fence_proxy_async_smem();
+          __syncwarp();
+          if (lane == 0) {
+            mbar_arrive(&bars[B_EMPTY + st]);
+            mbar_arrive(&bars[B_BFULL + b]);
+          }
+        }
+      }
+    }
+  } else {
+    // ------------------------------ epilogue ------------------------------
+    const int wq = warp & 3, half = (warp - G_W_EPI0) >> 2;
+    const int r = wq * 32 + lane;
+    float R[64];
+    long u = 0;
+    bool ok = true;
+    for (long t = blockIdx.x; ok && t < n_items; t += gridDim.x) {
+      const GrpItem it = grp_item(g, t);
+      for (int pidx = 0; ok && pidx < it.len; ++pidx) {
+        const GrpJob jb = grp_job(g, it, pidx);
+        const int tn = jb.tn, nch = tn / 8, per = (nch + 1) / 2;
+        const int c_begin = min(nch, half * per), c_end = min(nch, c_begin + per);
+        const int i = it.m0 + r;
+        const bool rok = i < jb.M;
+        const int jhi = min(tn, jb.N - it.n0);
+        float *crow = jb.C + (long)i * jb.ldc + it.n0;
+        const bool vec = ((reinterpret_cast<uintptr_t>(jb.C) & 15) == 0) && (jb.ldc & 3) == 0 &&
+                         (it.n0 & 3) == 0;
+#pragma unroll
+        for (int w = 0; w < 64; ++w) R[w] = 0.0f;
+        const int nchunks = (jb.nk + kc - 1) / kc;
+        for (int cu = 0; cu < nchunks; ++cu, ++u) {
+          const int a = (int)(u & 1);
+          if (!ws_wait(&bars[B_AFULL + a], (uint32_t)((u >> 1) & 1), s_abort, g.err)) {
+            ok = false;
+            break;
+          }
+          ptx::tc_fence_after();
+          const uint32_t acc_base = tmem + ((uint32_t)(wq * 32) << 16) + (uint32_t)(a * 256);
+#pragma unroll
+          for (int q = 0; q < 8; ++q) {
+            const int ch = c_begin + q;
+            if (ch < c_end) {
+              float dm[8], dc[8];
+              ptx::tmem_ld8(acc_base + ch * 8, dm);
+              ptx::tmem_ld8(acc_base + 128 + ch * 8, dc);
+              ptx::tmem_wait_ld();
+#pragma unroll
+              for (int w = 0; w < 8; ++w) R[q * 8 + w] += dm[w] + dc[w];
+            }
+          }
+          ptx::tc_fence_before();
+          __syncwarp();
+          if (lane == 0) mbar_arrive(&bars[B_AEMPTY + a]);
+        }
+        if (!ok || !rok) continue;
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+          const int ch = c_begin + q;
+          if (ch >= c_end) continue;
+          const int j0 = ch * 8;
+          if (j0 >= jhi) continue;
+          const float *v = R + q * 8;
+          if (vec && j0 + 8 <= jhi) {
+            float4 o0, o1;
+            if (jb.beta != 0.0f) {
+              const float4 c0 = *reinterpret_cast<const float4 *>(crow + j0);
+              const float4 c1 = *reinterpret_cast<const float4 *>(crow + j0 + 4);
+              o0 = make_float4(__fmaf_rn(jb.beta, c0.x, jb.alpha * v[0]),
+                               __fmaf_rn(jb.beta, c0.y, jb.alpha * v[1]),
+                               __fmaf_rn(jb.beta, c0.z, jb.alpha * v[2]),
+                               __fmaf_rn(jb.beta, c0.w, jb.alpha * v[3]));
+              o1 = make_float4(__fmaf_rn(jb.beta, c1.x, jb.alpha * v[4]),
+                               __fmaf_rn(jb.beta, c1.y, jb.alpha * v[5]),
+                               __fmaf_rn(jb.beta, c1.z, jb.alpha * v[6]),
+                               __fmaf_rn(jb.beta, c1.w, jb.alpha * v[7]));
+            } else {
+              o0 = make_float4(jb.alpha * v[0], jb.alpha * v[1], jb.alpha * v[2], jb.alpha * v[3]);
+              o1 = make_float4(jb.alpha * v[4], jb.alpha * v[5], jb.alpha * v[6], jb.alpha * v[7]);
+            }
+            *reinterpret_cast<float4 *>(crow + j0) = o0;
+            *reinterpret_cast<float4 *>(crow + j0 + 4) = o1;
+          } else {
+#pragma unroll
+            for (int w = 0; w < 8; ++w) {
+              if (j0 + w < jhi) {
+                float x = jb.alpha * v[w];
+                if (jb.beta != 0.0f) x = __fmaf_rn(jb.beta, crow[j0 + w], x);
+                crow[j0 + w] = x;
+              }
+            }
+          }
+        }
+      }
+    }
+  }
+
+  __syncthreads();
+  if (warp == G_W_MMA) {
+    ptx::tc_fence_after();
+    ptx::tmem_dealloc(tmem, WS_TMEM_COLS);
+  }
+}
+
 // device status word for the bounded waits
 __device__ unsigned g_tc_err;
 
@@ -1099,8 +1637,62 @@ int tc_sgemm_single(const GemmArgs<float> &g, int mode, int splits) {
   return tc_sgemm_strided(g, 0, 0, 0, 1, mode);
 }
 
-int tc_sgemm_grouped(const LibShalom_sgemm_entry *, long, int) {
-  return LIBSHALOM_ERR_UNSUPPORTED;
+int tc_sgemm_grouped(const LibShalom_sgemm_entry *entries, long count, int mode) {
+  if (!tc_mode_ok(mode)) return LIBSHALOM_ERR_INVALID_VALUE;
+  if (count > (1L << 30)) return LIBSHALOM_ERR_UNSUPPORTED;
+  State &st = state();
+  // plan workspace: 256-word header (class tables, run count), then three
+  // arrays sized by the entry count
+  const size_t words = 256 + 3 * (size_t)count + 1;
+  void *ws = nullptr;
+  int rc = workspace(words * sizeof(unsigned), &ws);
+  if (rc) return rc;
+  unsigned *w = static_cast<unsigned *>(ws);
+  GrpPlan pl;
+  pl.class_runs = w;
+  pl.class_off = w + GRP_CLASSES;
+  pl.class_fill = w + 2 * GRP_CLASSES;
+  pl.n_runs = w + 3 * GRP_CLASSES;
+  pl.run_first = w + 256;
+  pl.run_len = pl.run_first + count;
+  pl.tile_prefix = pl.run_len + count;
+  LS_CUDA_TRY(cudaMemsetAsync(w, 0, 256 * sizeof(unsigned), st.stream));
+  const int pgrid = (int)std::max(1L, std::min(cdiv(count, 256), (long)st.num_sms * 8));
+  k_grp_count<<<pgrid, 256, 0, st.stream>>>(entries, count, pl);
+  k_grp_offsets<<<1, 32, 0, st.stream>>>(pl);
+  k_grp_place<<<pgrid, 256, 0, st.stream>>>(entries, count, pl);
+  k_grp_prefix<<<1, 1024, 0, st.stream>>>(entries, pl);
+  LS_CUDA_TRY(cudaGetLastError());
+
+  void *errp = nullptr;
+  LS_CUDA_TRY(cudaGetSymbolAddress(&errp, g_tc_err));
+  GrpArgs g;
+  g.entries = entries;
+  g.count = count;
+  g.run_first = pl.run_first;
+  g.run_len = pl.run_len;
+  g.tile_prefix = pl.tile_prefix;
+  g.n_runs = pl.n_runs;
+  g.err = reinterpret_cast<unsigned *>(errp);
+  g.kc_slabs = 128 / TC_BK;
+  const void *kern = mode == LIBSHALOM_PREC_BF16X6 ? (const void *)k_tc_grouped<3>
+                                                   : (const void *)k_tc_grouped<2>;
+  (void)occupancy_of(kern, G_THREADS, WS_SMEM, 1);  // raises the shared-memory limit
+  const int grid = grid_for((long)st.num_sms, 1);
+  void *args[] = {&g};
+  LS_CUDA_TRY(cudaLaunchKernel(kern, dim3(grid), dim3(G_THREADS), args, WS_SMEM, st.stream));
+  LS_CUDA_TRY(cudaGetLastError());
+  if (st.sync) {
+    unsigned err = 0;
+    LS_CUDA_TRY(cudaStreamSynchronize(st.stream));
+    LS_CUDA_TRY(cudaMemcpyFromSymbol(&err, g_tc_err, sizeof(err)));
+    if (err) {
+      const unsigned zero = 0;
+      LS_CUDA_TRY(cudaMemcpyToSymbol(g_tc_err, &zero, sizeof(zero)));
+      return LIBSHALOM_ERR_DEVICE_TIMEOUT;
+    }
+  }
+  return LIBSHALOM_SUCCESS;
 }
 
 }  // namespace ls

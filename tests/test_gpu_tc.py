@@ -100,3 +100,93 @@ def test_tc_large_batch_spot_check(mode_setter, staging):
     A, B, _, C = _strided(ls.PREC_BF16X6, 0, n, n, n, count, seed=9)
     for g in (0, 1, 2, 1499, 2998, 2999):
         _check(C[g], A[g], B[g], 0, ls.PREC_BF16X6)
+
+
+# ---------------------------------------------------------------------------
+# grouped batches (LibShalom_sgemm_batched) on the tensor cores
+# ---------------------------------------------------------------------------
+from tests.test_gpu_plain import _sgemm_entries, _split  # noqa: E402
+
+
+@pytest.mark.parametrize("mode", [ls.PREC_BF16X6, ls.PREC_BF16X3])
+def test_tc_grouped_mixed_log_uniform(mode, mode_setter):
+    rng = np.random.default_rng(21)
+    shapes = []
+    for _ in range(400):
+        M, N, K = (int(np.exp(rng.uniform(np.log(4), np.log(256)))) for _ in range(3))
+        shapes.append((M, N, K, int(rng.integers(2))))
+    b = _sgemm_entries(shapes, beta_choices=(0.0, 1.0))
+    ls.set_precision(mode)
+    ls.sgemm_batched(b["dE"], len(shapes))
+    Cs = _split(to_host(b["dC"]), shapes)
+    for i, (M, N, K, tb) in enumerate(shapes):
+        ref = orc.sgemm_f64(b["As"][i], b["Bs"][i], tb, beta=b["betas"][i], C=b["C0s"][i])
+        assert normwise_err(Cs[i], ref) <= TOL[mode][0], (i, M, N, K, tb)
+
+
+def test_tc_grouped_large_and_long_k(mode_setter):
+    shapes = [(300, 200, 700, 0), (130, 257, 129, 1), (5, 300, 1000, 0), (256, 256, 256, 1),
+              (1, 1, 1, 0), (7, 3, 2000, 1)]
+    b = _sgemm_entries(shapes, beta_choices=(1.0,))
+    ls.set_precision(ls.PREC_BF16X6)
+    ls.sgemm_batched(b["dE"], len(shapes))
+    Cs = _split(to_host(b["dC"]), shapes)
+    for i, (M, N, K, tb) in enumerate(shapes):
+        ref = orc.sgemm_f64(b["As"][i], b["Bs"][i], tb, beta=1.0, C=b["C0s"][i])
+        assert normwise_err(Cs[i], ref) <= 1e-6, (i, M, N, K)
+
+
+def test_tc_grouped_runs_share_c(mode_setter):
+    """consecutive entries naming the same C are applied in order (C += A_p B_p)"""
+    import torch
+    sdt, _ = ls.entry_dtypes()
+    rng = np.random.default_rng(4)
+    runs = [(24, 40, [16, 33, 7]), (130, 20, [64, 64]), (9, 9, [5] * 8)]
+    As, Bs, C0 = [], [], []
+    for (M, N, Ks) in runs:
+        C0.append(orc.uniform_f32(len(C0) + 50, M * N))
+        for K in Ks:
+            As.append(orc.uniform_f32(len(As) + 100, M * K))
+            Bs.append(orc.uniform_f32(len(Bs) + 200, K * N))
+    dA = to_dev(np.concatenate(As))
+    dB = to_dev(np.concatenate(Bs))
+    dC = to_dev(np.concatenate(C0))
+    ent, oa, ob, oc, p = [], 0, 0, 0, 0
+    for (M, N, Ks) in runs:
+        for K in Ks:
+            ent.append((dA.data_ptr() + 4 * oa, dB.data_ptr() + 4 * ob, dC.data_ptr() + 4 * oc,
+                        M, N, K, 0, 0, 0, 0, 1.0, 1.0, 0))
+            oa += M * K
+            ob += K * N
+            p += 1
+        oc += M * N
+    arr = np.array(ent, sdt)
+    ls.set_precision(ls.PREC_BF16X6)
+    ls.sgemm_batched(torch.from_numpy(arr.view(np.uint8)).cuda(), len(arr))
+    got = to_host(dC)
+    oc, p = 0, 0
+    for r, (M, N, Ks) in enumerate(runs):
+        ref = C0[r].reshape(M, N).astype(np.float64)
+        for K in Ks:
+            ref = ref + As[p].reshape(M, K).astype(np.float64) @ Bs[p].reshape(K, N).astype(np.float64)
+            p += 1
+        assert normwise_err(got[oc:oc + M * N].reshape(M, N), ref) <= 1e-6, r
+        oc += M * N
+
+
+def test_tc_grouped_unaligned_leading_dims(mode_setter):
+    import torch
+    sdt, _ = ls.entry_dtypes()
+    M, N, K = 37, 29, 45
+    lda, ldb, ldc = 47, 31, 33   # not multiples of 4: the 4-byte copy path
+    A = orc.uniform_f32(1, M * lda).reshape(M, lda)
+    B = orc.uniform_f32(2, K * ldb).reshape(K, ldb)
+    C = np.zeros((M, ldc), np.float32)
+    dA, dB, dC = to_dev(A), to_dev(B), to_dev(C)
+    arr = np.array([(dA.data_ptr() + 4, dB.data_ptr(), dC.data_ptr(), M, N, K, 0, lda, ldb, ldc,
+                     1.0, 0.0, 0)], sdt)
+    ls.set_precision(ls.PREC_BF16X6)
+    ls.sgemm_batched(torch.from_numpy(arr.view(np.uint8)).cuda(), 1)
+    got = to_host(dC)[:, :N]
+    ref = orc.sgemm_f64(A[:, 1:1 + K], B[:, :N], 0)
+    assert normwise_err(got, ref) <= 1e-6
