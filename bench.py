@@ -58,6 +58,9 @@ def parse():
     p.add_argument("--mode", default="auto", choices=["auto", "fp32", "bf16x3", "bf16x6"])
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu", action="store_true")
+    p.add_argument("--workload", default="cube-sweep",
+                   choices=["cube-sweep", "single", "irregular", "dgemm-runs", "mixed"],
+                   help="cube-sweep is the headline; the others measure the other shapes")
     # smaller cases of the same workload, for profiling (not the bench line)
     p.add_argument("--sizes", default=None, help="comma list of cube sizes (default 8..128)")
     p.add_argument("--batch", type=int, default=None, help="GEMMs per size (default 10000)")
@@ -419,9 +422,277 @@ def run_gpu(args):
     return 0
 
 
+# --------------------------------------------------------------------------
+# secondary workloads (--workload): the other shapes the library is measured
+# on.  Same JSON contract; the default workload above is the headline.
+# --------------------------------------------------------------------------
+
+def _gpu_setup():
+    import torch
+    import libshalom_b200 as ls
+    torch.cuda.set_device(0)
+    s = torch.cuda.Stream()
+    ls.set_stream(s)
+    ls.set_sync(False)
+    return torch, ls, s
+
+
+def _time_events(torch, s, fn, steps, warmup):
+    for _ in range(warmup):
+        fn()
+    s.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(s)
+    for _ in range(steps):
+        fn()
+    e1.record(s)
+    s.synchronize()
+    return e0.elapsed_time(e1) / steps
+
+
+def _peak_hbm():
+    try:
+        return float(json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))["hbm_gbs"]), "measured"
+    except (OSError, ValueError, KeyError):
+        return 6650.0, "fallback"
+
+
+def _emit(metric, value, unit, ms, args, config, alg_bytes, extra):
+    peak, src = _peak_hbm()
+    gbs = alg_bytes / (ms / 1e3) / 1e9
+    line = {"metric": metric, "value": value, "unit": unit, "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "data": "synthetic", "config": config,
+            "roofline": {"bound": "hbm", "achieved": gbs, "peak": peak, "unit": "GB/s",
+                         "frac": gbs / peak, "traffic": None, "peak_source": src},
+            "e2e": None, "cpu_baseline": None}
+    line.update(extra)
+    print(json.dumps(line), flush=True)
+
+
+def wl_single(args):
+    """LibShalom_sgemm(NoTrans, Trans), M = N = K = 80, reference generator seed 0."""
+    torch, ls, s = _gpu_setup()
+    g = torch.Generator(device="cuda")
+    g.manual_seed(0)
+    A = torch.rand((80, 80), generator=g, device="cuda") * 2 - 1
+    B = torch.rand((80, 80), generator=g, device="cuda") * 2 - 1
+    C = torch.empty((80, 80), device="cuda")
+    flops = 2.0 * 80 ** 3
+    ms_async = _time_events(torch, s, lambda: ls.sgemm(0, 1, C, A, B, 80, 80, 80), args.steps,
+                            args.warmup)
+    ls.set_sync(True)
+    for _ in range(args.warmup):
+        ls.sgemm(0, 1, C, A, B, 80, 80, 80)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        ls.sgemm(0, 1, C, A, B, 80, 80, 80)
+    ms_sync = (time.perf_counter() - t0) / args.steps * 1e3
+    ls.set_sync(False)
+    _emit("single SGEMM NT 80^3 GFLOP/s (synchronous calls, as the reference API)",
+          flops / (ms_sync / 1e3) / 1e9, "GFLOP/s", ms_sync, args,
+          {"workload": "LibShalom_sgemm(NoTrans, Trans) M=N=K=80, C overwritten, one call per step"},
+          4.0 * 3 * 80 * 80,
+          {"dtype": "f32", "latency_us_sync": ms_sync * 1e3, "latency_us_stream": ms_async * 1e3,
+           "gflops_stream_ordered": flops / (ms_async / 1e3) / 1e9, "gpu_launches": args.steps})
+
+
+IRREGULAR = [(64, 3136, 576), (128, 784, 1152), (256, 196, 2304), (512, 49, 4608),
+             (20480, 32, 20480), (32, 20480, 4096)]
+
+
+def wl_irregular(args):
+    """LibShalom_sgemm_mp on the six tall-skinny / im2col shapes, NN."""
+    torch, ls, s = _gpu_setup()
+    g = torch.Generator(device="cuda")
+    g.manual_seed(3)
+    bufs = []
+    for (M, N, K) in IRREGULAR:
+        A = torch.rand((M, K), generator=g, device="cuda") * 2 - 1
+        B = torch.rand((K, N), generator=g, device="cuda") * 2 - 1
+        bufs.append((M, N, K, A, B, torch.empty((M, N), device="cuda")))
+    res = {}
+    modes = {"fp32_splitk_auto": (ls.PREC_FP32, 0), "fp32_reference_order": (ls.PREC_FP32, 1),
+             "bf16x6": (ls.PREC_BF16X6, 0), "bf16x3": (ls.PREC_BF16X3, 0)}
+    for name, (prec, split) in modes.items():
+        ls.set_precision(prec)
+        ls.set_splitk(split)
+        per = {}
+        tot_ms = 0.0
+        for (M, N, K, A, B, C) in bufs:
+            ms = _time_events(torch, s, lambda: ls.sgemm_mp(0, 0, C, A, B, M, N, K),
+                              args.steps, args.warmup)
+            ref = A.double() @ B.double()
+            err = ((C.double() - ref).abs().max() / ref.abs().max()).item()
+            per[f"{M}x{N}x{K}"] = {"ms": ms, "gflops": 2.0 * M * N * K / (ms / 1e3) / 1e9,
+                                   "max_normwise_err": err}
+            tot_ms += ms
+        flops = sum(2.0 * M * N * K for (M, N, K) in IRREGULAR)
+        res[name] = {"gflops": flops / (tot_ms / 1e3) / 1e9, "ms_all_shapes": tot_ms,
+                     "shapes": per}
+    ls.set_precision(ls.PREC_FP32)
+    ls.set_splitk(0)
+    ok = {k: v for k, v in res.items()
+          if max(x["max_normwise_err"] for x in v["shapes"].values()) <= 1e-6}
+    best = max(ok, key=lambda k: ok[k]["gflops"])
+    alg_bytes = sum(4.0 * (M * K + K * N + M * N) for (M, N, K) in IRREGULAR)
+    _emit("irregular SGEMM (sgemm_mp) aggregate GFLOP/s over the six shapes",
+          res[best]["gflops"], "GFLOP/s", res[best]["ms_all_shapes"], args,
+          {"workload": "LibShalom_sgemm_mp NN on (64,3136,576) (128,784,1152) (256,196,2304) "
+                       "(512,49,4608) (20480,32,20480) (32,20480,4096)", "mode": best},
+          alg_bytes, {"dtype": "f32", "modes": res, "gpu_launches": None})
+
+
+DGEMM_SIZES = [5, 9, 13, 16, 22, 23, 26, 32]
+
+
+def wl_dgemm_runs(args, count=200_000, run=8):
+    """LibShalom_dgemm_batched: C += A B, runs of 8 products share C."""
+    torch, ls, s = _gpu_setup()
+    rng = np.random.default_rng(7)
+    nruns = count // run
+    sz = np.array(DGEMM_SIZES)
+    Mr = sz[rng.integers(len(sz), size=nruns)]
+    Nr = sz[rng.integers(len(sz), size=nruns)]
+    M = np.repeat(Mr, run)
+    N = np.repeat(Nr, run)
+    K = sz[rng.integers(len(sz), size=count)]
+    a_len, b_len, c_len = M * K, K * N, Mr * Nr
+    offA = np.concatenate([[0], np.cumsum(a_len)[:-1]])
+    offB = np.concatenate([[0], np.cumsum(b_len)[:-1]])
+    offC_run = np.concatenate([[0], np.cumsum(c_len)[:-1]])
+    offC = np.repeat(offC_run, run)
+    g = torch.Generator(device="cuda")
+    g.manual_seed(11)
+    # entries: normal(0,1) * 10^u with u ~ U[-3, 3] drawn once per matrix
+    uA = torch.from_numpy(np.repeat(10.0 ** rng.uniform(-3, 3, count), a_len)).cuda()
+    uB = torch.from_numpy(np.repeat(10.0 ** rng.uniform(-3, 3, count), b_len)).cuda()
+    dA = torch.randn(int(a_len.sum()), generator=g, device="cuda", dtype=torch.float64) * uA
+    dB = torch.randn(int(b_len.sum()), generator=g, device="cuda", dtype=torch.float64) * uB
+    del uA, uB
+    dC0 = torch.randn(int(c_len.sum()), generator=g, device="cuda", dtype=torch.float64)
+    dC = dC0.clone()
+    _, ddt = ls.entry_dtypes()
+    ent = np.zeros(count, ddt)
+    ent["A"] = dA.data_ptr() + 8 * offA
+    ent["B"] = dB.data_ptr() + 8 * offB
+    ent["C"] = dC.data_ptr() + 8 * offC
+    ent["M"], ent["N"], ent["K"] = M, N, K
+    ent["alpha"] = 1.0
+    ent["beta"] = 1.0
+    dE = torch.from_numpy(ent.view(np.uint8)).cuda()
+    flops = float(2.0 * (M * N * K).sum())
+    alg_bytes = float(8.0 * (a_len.sum() + b_len.sum() + 2 * c_len.sum()))
+    ms = _time_events(torch, s, lambda: ls.dgemm_batched(dE, count), args.steps, args.warmup)
+    # per-call plain FP64 kernel over a sample of the same products
+    sample = 4000
+    C1 = dC.clone()
+
+    def percall():
+        for i in range(sample):
+            ls.dgemm(0, 0, C1.data_ptr() + 8 * int(offC[i]), dA.data_ptr() + 8 * int(offA[i]),
+                     dB.data_ptr() + 8 * int(offB[i]), int(M[i]), int(N[i]), int(K[i]))
+    ms_pc = _time_events(torch, s, percall, 1, 1)
+    pc_gflops = float(2.0 * (M[:sample] * N[:sample] * K[:sample]).sum()) / (ms_pc / 1e3) / 1e9
+    value = flops / (ms / 1e3) / 1e9
+    _emit("batched uneven DGEMM GFLOP/s (200,000 products, runs of 8 share C)", value, "GFLOP/s",
+          ms, args,
+          {"workload": "LibShalom_dgemm_batched, C += A B, M,N per run and K per product from "
+                       "{5,9,13,16,22,23,26,32}, entries normal(0,1)*10^u, u~U[-3,3] per matrix",
+           "products": count, "run": run, "step_gflop": flops / 1e9, "step_gbytes": alg_bytes / 1e9},
+          alg_bytes,
+          {"dtype": "f64", "gpu_launches": 2 * args.steps,
+           "per_call_plain_fp64": {"gflops": pc_gflops, "sample_products": sample,
+                                   "note": "loop of LibShalom_dgemm (overwrite semantics) on the "
+                                           "first products, stream-ordered"},
+           "speedup_vs_per_call": value / pc_gflops})
+
+
+def wl_mixed(args, count=50_000):
+    """LibShalom_sgemm_batched: log-uniform M, N, K in [4, 256], NN/NT, beta 0/1."""
+    torch, ls, s = _gpu_setup()
+    rng = np.random.default_rng(5)
+    dims = np.exp(rng.uniform(np.log(4), np.log(256), size=(count, 3))).astype(np.int64)
+    M, N, K = dims[:, 0], dims[:, 1], dims[:, 2]
+    tb = rng.integers(2, size=count)
+    beta = rng.integers(2, size=count).astype(np.float32)
+    a_len, b_len, c_len = M * K, K * N, M * N
+    offs = [np.concatenate([[0], np.cumsum(x)[:-1]]) for x in (a_len, b_len, c_len)]
+    g = torch.Generator(device="cuda")
+    g.manual_seed(13)
+    dA = torch.rand(int(a_len.sum()), generator=g, device="cuda") * 2 - 1
+    dB = torch.rand(int(b_len.sum()), generator=g, device="cuda") * 2 - 1
+    dC0 = torch.rand(int(c_len.sum()), generator=g, device="cuda") * 2 - 1
+    dC = dC0.clone()
+    sdt, _ = ls.entry_dtypes()
+    ent = np.zeros(count, sdt)
+    ent["A"] = dA.data_ptr() + 4 * offs[0]
+    ent["B"] = dB.data_ptr() + 4 * offs[1]
+    ent["C"] = dC.data_ptr() + 4 * offs[2]
+    ent["M"], ent["N"], ent["K"], ent["transb"] = M, N, K, tb
+    ent["alpha"] = 1.0
+    ent["beta"] = beta
+    dE = torch.from_numpy(ent.view(np.uint8)).cuda()
+    flops = float(2.0 * (M * N * K).sum())
+    alg_bytes = float(4.0 * (a_len.sum() + b_len.sum() + c_len.sum() * (1 + beta).astype(np.int64)))
+    res = {}
+    for name, prec in (("bf16x6", ls.PREC_BF16X6), ("bf16x3", ls.PREC_BF16X3),
+                       ("fp32", ls.PREC_FP32)):
+        ls.set_precision(prec)
+        dC.copy_(dC0)
+        ls.sgemm_batched(dE, count)
+        s.synchronize()
+        # error on a sample against FP64 (beta applied to the original C)
+        err = 0.0
+        for i in range(0, count, count // 200):
+            a = dA[offs[0][i]:offs[0][i] + a_len[i]].double().view(int(M[i]), int(K[i]))
+            bb = dB[offs[1][i]:offs[1][i] + b_len[i]].double()
+            bm = bb.view(int(N[i]), int(K[i])).t() if tb[i] else bb.view(int(K[i]), int(N[i]))
+            ref = a @ bm + float(beta[i]) * dC0[offs[2][i]:offs[2][i] + c_len[i]].double().view(
+                int(M[i]), int(N[i]))
+            got = dC[offs[2][i]:offs[2][i] + c_len[i]].double().view(int(M[i]), int(N[i]))
+            err = max(err, ((got - ref).abs().max() / ref.abs().max()).item())
+        ms = _time_events(torch, s, lambda: ls.sgemm_batched(dE, count), args.steps, args.warmup)
+        res[name] = {"gflops": flops / (ms / 1e3) / 1e9, "ms": ms, "max_normwise_err": err}
+    # the same batch replayed from a captured CUDA graph
+    ls.set_precision(ls.PREC_BF16X6)
+    graph = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(graph, stream=s):
+        ls.sgemm_batched(dE, count)
+    ms_graph = _time_events(torch, s, graph.replay, args.steps, args.warmup)
+    res["bf16x6_graph"] = {"gflops": flops / (ms_graph / 1e3) / 1e9, "ms": ms_graph}
+    # looping plain FP32 per-call kernels over a sample
+    sample = 5000
+    ls.set_precision(ls.PREC_FP32)
+
+    def percall():
+        for i in range(sample):
+            ls.sgemm_batched_strided(int(tb[i]), int(M[i]), int(N[i]), int(K[i]), 1.0,
+                                     dA.data_ptr() + 4 * int(offs[0][i]), 0,
+                                     dB.data_ptr() + 4 * int(offs[1][i]), 0, float(beta[i]),
+                                     dC.data_ptr() + 4 * int(offs[2][i]), 0, 1)
+    ms_pc = _time_events(torch, s, percall, 1, 1)
+    pc = float(2.0 * (M[:sample] * N[:sample] * K[:sample]).sum()) / (ms_pc / 1e3) / 1e9
+    res["per_call_fp32"] = {"gflops": pc, "sample_gemms": sample}
+    ls.set_precision(ls.PREC_FP32)
+    best = "bf16x6"
+    _emit("mixed uneven SGEMM batch GFLOP/s (50,000 GEMMs, log-uniform 4..256)",
+          res[best]["gflops"], "GFLOP/s", res[best]["ms"], args,
+          {"workload": "LibShalom_sgemm_batched, M,N,K log-uniform integers in [4,256], "
+                       "NN/NT 50/50, alpha 1, beta 0/1", "gemms": count, "mode": best,
+           "step_gflop": flops / 1e9, "step_gbytes": alg_bytes / 1e9},
+          alg_bytes,
+          {"dtype": "f32 (bf16 split products, f32 accumulate)", "modes": res,
+           "speedup_vs_per_call": res[best]["gflops"] / pc, "gpu_launches": 6 * args.steps})
+
+
 def main():
     global SIZES, BATCH, LAYOUTS
     args = parse()
+    if args.workload != "cube-sweep" and args.impl != "reference":
+        return {"single": wl_single, "irregular": wl_irregular, "dgemm-runs": wl_dgemm_runs,
+                "mixed": wl_mixed}[args.workload](args) or 0
     if args.sizes:
         SIZES = [int(x) for x in args.sizes.split(",")]
     if args.batch:

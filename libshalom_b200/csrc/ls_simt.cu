@@ -401,7 +401,14 @@ static int launch_grouped(const typename EntryOf<T>::type *entries, long count, 
 int run_grouped_s(const LibShalom_sgemm_entry *entries, long count) {
   return launch_grouped<float, S64>(entries, count, 4);
 }
+// Grouped FP64 batches go to the run kernel of ls_dgemm.cu (C tile held in
+// registers across a run, cp.async double buffer); the generic tile kernel
+// above stays available for comparison.
 int run_grouped_d(const LibShalom_dgemm_entry *entries, long count) {
+  return run_dgemm_runs(entries, count);
+}
+
+int run_grouped_d_generic(const LibShalom_dgemm_entry *entries, long count) {
   return launch_grouped<double, D32>(entries, count, 4);
 }
 

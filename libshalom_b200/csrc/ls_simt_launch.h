@@ -27,6 +27,9 @@ int run_strided(const GemmArgs<T> &g, long sA, long sB, long sC, long count);
 
 int run_grouped_s(const LibShalom_sgemm_entry *entries, long count);
 int run_grouped_d(const LibShalom_dgemm_entry *entries, long count);
+int run_grouped_d_generic(const LibShalom_dgemm_entry *entries, long count);
+// ls_dgemm.cu: runs of products sharing C, C tile held in registers
+int run_dgemm_runs(const LibShalom_dgemm_entry *entries, long count);
 
 // Plain FP32 split-K GEMM (GEMM_K-aligned slices, rounding order of the mp
 // path per slice) with the partial sums in `partial` (>= splits * M * N
