@@ -71,6 +71,23 @@ def parse():
     return p.parse_args()
 
 
+def max_over_ranks(ms, world, device):
+    """Slowest rank's time: every replica processes the same work, so the job
+    takes as long as its slowest rank (no data-path collective)."""
+    if world <= 1:
+        return float(ms)
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(ms)], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def whole_job_rate(flops_per_rank, ms, world):
+    """Aggregate GFLOP/s of `world` replicas that each did flops_per_rank in ms."""
+    return world * flops_per_rank / (ms / 1e3) / 1e9
+
+
 def dist_env():
     return (int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")),
             int(os.environ.get("LOCAL_RANK", "0")))
@@ -321,12 +338,8 @@ def run_gpu(args):
     time.sleep(0.5)  # nvidia-smi needs a moment before its first sample
     total_ms, kern_ms = timed(best)
     clk = clocks.stop()
-    ms_step = total_ms / args.steps
-    if world > 1:
-        t = torch.tensor([ms_step], device=dev)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        ms_step = t.item()
-    value = world * step_flops() / (ms_step / 1e3) / 1e9
+    ms_step = max_over_ranks(total_ms / args.steps, world, dev)
+    value = whole_job_rate(step_flops(), ms_step, world)
     launches = args.steps * len(bufs)
     kern_ms_per_launch = kern_ms / launches
     achieved_gbs = step_bytes() / len(bufs) / (kern_ms_per_launch / 1e3) / 1e9
@@ -375,12 +388,8 @@ def run_gpu(args):
                 e2e_step()
             s1.record(stream)
             stream.synchronize()
-        e_ms = s0.elapsed_time(s1) / e_steps
-        if world > 1:
-            t = torch.tensor([e_ms], device=dev)
-            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-            e_ms = t.item()
-        e2e = {"value": world * step_flops() / (e_ms / 1e3) / 1e9, "unit": "GFLOP/s",
+        e_ms = max_over_ranks(s0.elapsed_time(s1) / e_steps, world, dev)
+        e2e = {"value": whole_job_rate(step_flops(), e_ms, world), "unit": "GFLOP/s",
                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "ms_per_step": e_ms}
 
     cpu = None
@@ -645,7 +654,7 @@ def wl_mixed(args, count=50_000):
     ent["beta"] = beta
     dE = torch.from_numpy(ent.view(np.uint8)).cuda()
     flops = float(2.0 * (M * N * K).sum())
-    alg_bytes = float(4.0 * (a_len.sum() + b_len.sum() + c_len.sum() * (1 + beta).astype(np.int64)))
+    alg_bytes = float(4.0 * (a_len.sum() + b_len.sum() + (c_len * (1 + beta)).sum()))
     res = {}
     for name, prec in (("bf16x6", ls.PREC_BF16X6), ("bf16x3", ls.PREC_BF16X3),
                        ("fp32", ls.PREC_FP32)):

@@ -352,6 +352,17 @@ int run_gemm_splitk_external(const GemmArgs<float> &g, int splits, float *partia
   return LIBSHALOM_SUCCESS;
 }
 
+int run_splitk_reduce_f32(const float *partial, int splits, long M, long N, float *C, long ldc,
+                          float alpha, float beta) {
+  State &st = state();
+  const long total = M * N;
+  const int grid = (int)std::min<long>(cdiv(total, 256), (long)st.num_sms * 8);
+  k_splitk_reduce<float><<<std::max(grid, 1), 256, 0, st.stream>>>(partial, splits, M, N, C, ldc,
+                                                                  alpha, beta);
+  LS_CUDA_TRY(cudaGetLastError());
+  return LIBSHALOM_SUCCESS;
+}
+
 template int run_gemm<float>(const GemmArgs<float> &, const SimtOptions &, SimtPlan *);
 template int run_gemm<double>(const GemmArgs<double> &, const SimtOptions &, SimtPlan *);
 

@@ -28,6 +28,9 @@ int run_strided(const GemmArgs<T> &g, long sA, long sB, long sC, long count);
 int run_grouped_s(const LibShalom_sgemm_entry *entries, long count);
 int run_grouped_d(const LibShalom_dgemm_entry *entries, long count);
 int run_grouped_d_generic(const LibShalom_dgemm_entry *entries, long count);
+// C = alpha * sum_z partial[z] + beta * C, partial slices summed in order
+int run_splitk_reduce_f32(const float *partial, int splits, long M, long N, float *C, long ldc,
+                          float alpha, float beta);
 // ls_dgemm.cu: runs of products sharing C, C tile held in registers
 int run_dgemm_runs(const LibShalom_dgemm_entry *entries, long count);
 

@@ -31,6 +31,7 @@
 
 #include "ls_common.cuh"
 #include "ls_tc_launch.h"
+#include "ls_simt_launch.h"
 #include "ls_tc_ptx.cuh"
 
 namespace ls {
@@ -82,6 +83,10 @@ struct TcProblem {
   int vec_a, vec_b;  // 16-byte cp.async allowed for A / B rows
   int vec_c;       // 16-byte stores allowed for C rows
   int kc_slabs;    // DRAIN kernels: slabs per TMEM accumulation chunk
+  // split-K of one GEMM: "GEMM" g of the batch is K slice g of a single
+  // product (A and B not offset; the slice's K range starts at g * kslice),
+  // written to partial C_g = C + g * sC; 0 = no split
+  int kslice;
   unsigned *err;   // device status word (bounded waits)
 };
 
@@ -663,10 +668,12 @@ __global__ void __launch_bounds__(WS_THREADS, 1)
           const uint32_t dst = smem_base + WS_OFF_STAGE + st * WS_STAGE_BYTES;
           mbar_arrive_tx(&bars[B_FULL + st], args.tx_bytes);
           const int k0 = s * TC_BK;
-          const int g = (int)ti.g0;
-          tma_load_3d(dst, &tmA, &bars[B_FULL + st], k0, ti.m0, g);
-          if (p.transb) tma_load_3d(dst + 16384, &tmB, &bars[B_FULL + st], k0, ti.n0, g);
-          else tma_load_3d(dst + 16384, &tmB, &bars[B_FULL + st], ti.n0, k0, g);
+          // split-K: slice g reads K range [g*kslice, (g+1)*kslice) of one matrix
+          const int g = p.kslice ? 0 : (int)ti.g0;
+          const int kk = k0 + (p.kslice ? (int)ti.g0 * p.kslice : 0);
+          tma_load_3d(dst, &tmA, &bars[B_FULL + st], kk, ti.m0, g);
+          if (p.transb) tma_load_3d(dst + 16384, &tmB, &bars[B_FULL + st], kk, ti.n0, g);
+          else tma_load_3d(dst + 16384, &tmB, &bars[B_FULL + st], ti.n0, kk, g);
         }
       }
     }
@@ -1512,7 +1519,8 @@ bool encode_map(CUtensorMap *map, const float *base, uint64_t d0, uint64_t d1, u
 // Tensor maps for the warp-specialized kernel, or false when TMA cannot
 // address the operands (unaligned base or row stride, overlapping batches).
 bool ws_maps(const TcProblem &p, CUtensorMap *ma, CUtensorMap *mb, WsArgs *wa) {
-  const long count = p.count;
+  // split-K slices all read the one matrix pair: a single-batch tensor map
+  const long count = p.kslice ? 1 : p.count;
   const long sA = count > 1 ? p.sA : (long)p.M * p.lda;
   const long rowsB = p.transb ? p.N : p.K;
   const long sB = count > 1 ? p.sB : rowsB * p.ldb;
@@ -1632,9 +1640,56 @@ int tc_sgemm_strided(const GemmArgs<float> &g, long sA, long sB, long sC, long c
   return tc_launch(p, mode);
 }
 
+// Split factor for one GEMM on the tensor cores: K is cut into s slices of
+// equal length (s divides K / 32, slices of at least 64 k) when the output
+// tiles alone cannot fill the machine.  forced > 1 asks for about that many.
+static int tc_pick_splits(const GemmArgs<float> &g, int forced) {
+  if (forced == 1 || g.K % TC_BK || g.K < 2 * TC_BK) return 1;
+  const long q = g.K / TC_BK;
+  const int tn = (int)std::min<long>(TC_MAX_N, cdiv(g.N, 16) * 16);
+  const long tiles = cdiv(g.M, TC_BM) * cdiv(g.N, tn);
+  const int sms = state().num_sms;
+  long want = forced > 1 ? forced : (tiles >= sms ? 1 : (2L * sms) / tiles);
+  want = std::min(want, q / 2);  // every slice keeps at least 2 slabs
+  for (long d = want; d > 1; --d)
+    if (q % d == 0) return (int)d;
+  return 1;
+}
+
 int tc_sgemm_single(const GemmArgs<float> &g, int mode, int splits) {
-  (void)splits;
-  return tc_sgemm_strided(g, 0, 0, 0, 1, mode);
+  if (!tc_mode_ok(mode)) return LIBSHALOM_ERR_INVALID_VALUE;
+  const int s = g.transa ? 1 : tc_pick_splits(g, splits);
+  if (s <= 1 || !state().use_tma) return tc_sgemm_strided(g, 0, 0, 0, 1, mode);
+  // K slices as a batch of s partial products into the workspace, then an
+  // ordered reduction C = alpha * sum_z partial_z + beta * C
+  void *ws = nullptr;
+  int rc = workspace(sizeof(float) * (size_t)s * g.M * g.N, &ws);
+  if (rc) return rc;
+  float *partial = static_cast<float *>(ws);
+  TcProblem p{};
+  p.A = g.A; p.B = g.B; p.C = partial;
+  p.sA = 0; p.sB = 0; p.sC = g.M * g.N;
+  p.M = (int)g.M; p.N = (int)g.N; p.K = (int)g.K;
+  p.lda = (int)g.lda; p.ldb = (int)g.ldb; p.ldc = (int)g.N;
+  p.transb = g.transb;
+  p.alpha = 1.0f; p.beta = 0.0f;
+  p.count = s;
+  p.G = 1;
+  p.tile_n = std::min(TC_MAX_N, (int)cdiv(p.N, 16) * 16);
+  p.tiles_m = (int)cdiv(p.M, TC_BM);
+  p.tiles_n = (int)cdiv(p.N, p.tile_n);
+  p.num_tiles = (long)p.tiles_m * p.tiles_n * s;
+  p.kslice = p.K / s;
+  p.nk = p.kslice / TC_BK;
+  p.kc_slabs = 128 / TC_BK;
+  p.vec_a = p.vec_b = 0;
+  p.vec_c = 1;
+  CUtensorMap ma, mb;
+  WsArgs wa;
+  if (!ws_maps(p, &ma, &mb, &wa)) return tc_sgemm_strided(g, 0, 0, 0, 1, mode);
+  rc = tc_launch(p, mode);
+  if (rc) return rc;
+  return run_splitk_reduce_f32(partial, s, g.M, g.N, g.C, g.ldc, g.alpha, g.beta);
 }
 
 int tc_sgemm_grouped(const LibShalom_sgemm_entry *entries, long count, int mode) {

@@ -190,3 +190,20 @@ def test_tc_grouped_unaligned_leading_dims(mode_setter):
     got = to_host(dC)[:, :N]
     ref = orc.sgemm_f64(A[:, 1:1 + K], B[:, :N], 0)
     assert normwise_err(got, ref) <= 1e-6
+
+
+@pytest.mark.parametrize("splits", [0, 3, 8])
+def test_tc_sgemm_mp_split_k(splits, mode_setter):
+    """K slices of one GEMM as a batch of partial products plus an ordered
+    reduction (auto choice, and forced factors that must divide K / 32)"""
+    import torch
+    M, N, K = 256, 196, 2304
+    A, B = orc.gemm_inputs_f32(99, M, N, K, 0)
+    dC = torch.full((M, N), float("nan"), device="cuda")
+    ls.set_precision(ls.PREC_BF16X6)
+    ls.set_splitk(splits)
+    try:
+        ls.sgemm_mp(0, 0, dC, to_dev(A), to_dev(B), M, N, K)
+    finally:
+        ls.set_splitk(0)
+    _check(to_host(dC), A, B, 0, ls.PREC_BF16X6)
