@@ -4,13 +4,17 @@
 // accumulate into the same C block (C += A_p B_p).
 //
 // Work unit: one run (maximal group of consecutive entries naming the same C)
-// and one 32 x 32 tile of its C block.  The CTA (256 threads, 4 outputs each)
-// loads the C tile once, applies the run's products in array order with the C
-// tile held in registers (C = alpha_p A_p op(B_p) + beta_p C), and writes it
-// once -- the owner-computes rule that keeps shared C blocks race-free and the
-// result deterministic without atomics.  Each product is a fused multiply-add
-// chain over k in increasing order (the reference's KERNEL7x6 order) followed
-// by C = fma(beta, C, alpha * acc).
+// and one 32 x 32 tile of its C block.  The CTA (128 threads, 2 x 4 outputs
+// each) loads the C tile once, applies the run's products in array order with
+// the C tile held in registers (C = alpha_p A_p op(B_p) + beta_p C), and writes
+// it once -- the owner-computes rule that keeps shared C blocks race-free and
+// the result deterministic without atomics.  A and op(B) arrive in 32 x 32
+// slabs through an 8-byte cp.async double buffer that prefetches the next slab
+// (of the same product, the next product or the next run) while the current
+// one is multiplied, staged transposed (A as [k][m]) so the inner loop reads
+// contiguous vectors.  Each product is a fused multiply-add chain over k in
+// increasing order (the reference's KERNEL7x6 order) followed by
+// C = fma(beta, C, alpha * acc).
 //
 // Runs are found on the device (k_drun_plan: one slot per run start), so the
 // call needs no host round trip.
@@ -25,7 +29,10 @@ namespace ls {
 
 namespace {
 
-constexpr int DR_T = 32;  // C tile edge
+constexpr int DR_THREADS = 128;
+constexpr int DR_T = 32;       // C tile edge and K slab
+constexpr int DR_P = 34;       // padded pitch (doubles) of the staged slabs
+constexpr int DR_STAGE = 2 * DR_T * DR_P;  // doubles per stage: A^T and B
 
 struct DrunPlan {
   unsigned *n_runs;
@@ -45,240 +52,182 @@ __global__ void k_drun_plan(const LibShalom_dgemm_entry *e, long count, DrunPlan
   }
 }
 
+struct DJob {
+  const double *A, *B;
+  int M, N, K, lda, ldb, transb;
+  double alpha, beta;
+};
+
+__device__ __forceinline__ DJob djob(const LibShalom_dgemm_entry &e) {
+  DJob j;
+  j.A = e.A; j.B = e.B;
+  j.M = e.M; j.N = e.N; j.K = max(0, e.K);
+  j.transb = e.transb;
+  j.lda = e.lda > 0 ? e.lda : j.K;
+  j.ldb = e.ldb > 0 ? e.ldb : (e.transb ? j.K : j.N);
+  j.alpha = e.alpha; j.beta = e.beta;
+  return j;
+}
+
 __device__ __forceinline__ void cp_async8(uint32_t saddr, const void *g) {
   asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(saddr), "l"(g) : "memory");
 }
+__device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
 template <int N>
 __device__ __forceinline__ void cp_wait() {
   asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
 }
 
-// ---------------------------------------------------------------------------
-// Ring-staged variant.  The CTA walks its sequence of items -- (run, 32 x 32
-// C tile, product, K slice of up to 64) -- with a producer cursor running up
-// to RG_Q items ahead of the consumer: every item's A and op(B) pieces are
-// copied (8-byte cp.async, exact sizes, compact layouts) into the next free
-// bytes of a 96 KB shared-memory ring, and each thread's copies arrive on the
-// item's mbarrier when they land (cp.async.mbarrier.arrive.noinc).  So many
-// small products are in flight at once instead of one fixed-size slab.  The
-// producer and consumer cursors compute the same placements (same rule), so
-// no queue is shared between them.
-// ---------------------------------------------------------------------------
-constexpr int RG_THREADS = 256;
-constexpr int RG_KS = 64;                  // K slice of an item
-constexpr int RG_RING = 96 * 1024;         // bytes
-constexpr int RG_Q = 16;                   // items in flight (mbarrier slots)
-constexpr int RG_SMEM = RG_RING + RG_Q * 8;
-
-struct RgCursor {
-  long r;       // run slot (round-robin over CTAs)
-  int t, p, k;  // C tile, product, K slice
-  bool valid;
+// Position in this CTA's sequence of slabs: run slot r (round-robin over the
+// CTAs), C tile t of the run, product p of the run, K slab k of the product.
+struct DCursor {
+  long r;
+  int t, p, k;
 };
 
-struct RgItem {
-  const double *A, *B;
-  int transb, lda, ldb;
-  int m0, n0, k0, mcnt, ncnt, kcnt;
-  int bytes;  // staged bytes (A then B), 16-byte rounded
-};
-
-__device__ __forceinline__ bool rg_mbar_try(uint64_t *bar, uint32_t parity) {
-  uint32_t ok;
-  asm volatile(
-      "{\n\t.reg .pred p;\n\t"
-      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-      "selp.b32 %0, 1, 0, p;\n\t}"
-      : "=r"(ok)
-      : "r"((uint32_t)__cvta_generic_to_shared(bar)), "r"(parity)
-      : "memory");
-  return ok != 0;
-}
-
-__global__ void __launch_bounds__(RG_THREADS, 2)
-    k_dgemm_ring(const LibShalom_dgemm_entry *entries, const unsigned *n_runs_p,
-                 const unsigned *run_first, const unsigned *run_len, unsigned *err) {
-  extern __shared__ __align__(16) unsigned char rsm[];
-  uint64_t *bars = reinterpret_cast<uint64_t *>(rsm + RG_RING);
+__global__ void __launch_bounds__(DR_THREADS, 4)
+    k_dgemm_runs(const LibShalom_dgemm_entry *entries, const unsigned *n_runs_p,
+                 const unsigned *run_first, const unsigned *run_len) {
+  __shared__ __align__(16) double stage[2][DR_STAGE];
   const int tid = threadIdx.x;
+  const int tx = tid & 7, ty = tid >> 3;  // outputs: rows 2ty, 2ty+1; cols 4tx..4tx+3
   const long n_runs = (long)*n_runs_p;
-  __shared__ int s_abort;
-  if (tid == 0) {
-    for (int i = 0; i < RG_Q; ++i)
-      asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(
-                       (uint32_t)__cvta_generic_to_shared(&bars[i])),
-                   "r"(RG_THREADS));
-    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-    s_abort = 0;
-  }
-  __syncthreads();
 
   auto tiles_of = [&](const LibShalom_dgemm_entry &e) {
-    return (e.M > 0 && e.N > 0) ? ((e.M + DR_T - 1) / DR_T) * ((e.N + DR_T - 1) / DR_T) : 0;
+    return ((e.M + DR_T - 1) / DR_T) * ((e.N + DR_T - 1) / DR_T);
   };
-  auto kslices_of = [&](const LibShalom_dgemm_entry &e) {
-    return max(1, (max(0, e.K) + RG_KS - 1) / RG_KS);
-  };
-  auto first = [&](RgCursor &c) {
-    c.t = c.p = c.k = 0;
-    for (c.r = blockIdx.x; c.r < n_runs; c.r += gridDim.x)
-      if (tiles_of(entries[run_first[c.r]]) > 0) { c.valid = true; return; }
-    c.valid = false;
-  };
-  auto advance = [&](RgCursor &c) {
-    if (!c.valid) return;
+  auto slabs_of = [&](const LibShalom_dgemm_entry &e) { return max(1, (max(0, e.K) + DR_T - 1) / DR_T); };
+
+  // advance a cursor to the next slab; returns false past the CTA's last run
+  auto advance = [&](DCursor &c) -> bool {
+    if (c.r >= n_runs) return false;
     const unsigned f = run_first[c.r], len = run_len[c.r];
-    if (++c.k < kslices_of(entries[f + c.p])) return;
+    if (++c.k < slabs_of(entries[f + c.p])) return true;
     c.k = 0;
-    if (++c.p < (int)len) return;
+    if (++c.p < (int)len) return true;
     c.p = 0;
-    if (++c.t < tiles_of(entries[f])) return;
+    if (++c.t < tiles_of(entries[f])) return true;
     c.t = 0;
     for (c.r += gridDim.x; c.r < n_runs; c.r += gridDim.x)
-      if (tiles_of(entries[run_first[c.r]]) > 0) return;
-    c.valid = false;
+      if (tiles_of(entries[run_first[c.r]]) > 0) return true;
+    return false;
   };
-  auto item_of = [&](const RgCursor &c) {
+  auto first = [&](DCursor &c) -> bool {
+    c.t = c.p = c.k = 0;
+    for (c.r = blockIdx.x; c.r < n_runs; c.r += gridDim.x)
+      if (tiles_of(entries[run_first[c.r]]) > 0) return true;
+    return false;
+  };
+
+  // issue the cp.async copies of the slab at cursor c into stage buffer b
+  auto load = [&](const DCursor &c, int b) {
     const unsigned f = run_first[c.r];
     const LibShalom_dgemm_entry &e0 = entries[f];
-    const LibShalom_dgemm_entry &e = entries[f + c.p];
-    RgItem it;
-    const int K = max(0, e.K);
-    it.A = e.A; it.B = e.B;
-    it.transb = e.transb;
-    it.lda = e.lda > 0 ? e.lda : K;
-    it.ldb = e.ldb > 0 ? e.ldb : (e.transb ? K : e0.N);
+    const DJob jb = djob(entries[f + c.p]);
     const int tiles_n = (e0.N + DR_T - 1) / DR_T;
-    it.m0 = (c.t / tiles_n) * DR_T;
-    it.n0 = (c.t % tiles_n) * DR_T;
-    it.k0 = c.k * RG_KS;
-    it.mcnt = min(DR_T, e0.M - it.m0);
-    it.ncnt = min(DR_T, e0.N - it.n0);
-    it.kcnt = max(0, min(RG_KS, K - it.k0));
-    it.bytes = ((it.mcnt + it.ncnt) * it.kcnt * 8 + 15) & ~15;
-    return it;
+    const int m0 = (c.t / tiles_n) * DR_T, n0 = (c.t % tiles_n) * DR_T, k0 = c.k * DR_T;
+    double *As = stage[b];
+    double *Bs = stage[b] + DR_T * DR_P;
+    const uint32_t sa = (uint32_t)__cvta_generic_to_shared(As);
+    const uint32_t sb = (uint32_t)__cvta_generic_to_shared(Bs);
+#pragma unroll
+    for (int q = 0; q < (DR_T * DR_T) / DR_THREADS; ++q) {
+      const int e = tid + q * DR_THREADS;
+      // A element (m, k): consecutive threads take consecutive k (contiguous in memory)
+      const int m = e >> 5, k = e & 31;
+      if (m0 + m < jb.M && k0 + k < jb.K)
+        cp_async8(sa + (k * DR_P + m) * 8, jb.A + (long)(m0 + m) * jb.lda + k0 + k);
+      // B element (k, n) of op(B)
+      if (!jb.transb) {
+        const int kk = e >> 5, n = e & 31;
+        if (k0 + kk < jb.K && n0 + n < jb.N)
+          cp_async8(sb + (kk * DR_P + n) * 8, jb.B + (long)(k0 + kk) * jb.ldb + n0 + n);
+      } else {
+        const int n = e >> 5, kk = e & 31;
+        if (k0 + kk < jb.K && n0 + n < jb.N)
+          cp_async8(sb + (kk * DR_P + n) * 8, jb.B + (long)(n0 + n) * jb.ldb + k0 + kk);
+      }
+    }
   };
-  // placement rule shared by producer and consumer: an item never wraps
-  auto place = [&](long &head, int bytes) -> int {
-    long off = head % RG_RING;
-    if (off + bytes > RG_RING) {
-      head += RG_RING - off;
-      off = 0;
-    }
-    head += bytes;
-    return (int)off;
-  };
 
-  RgCursor pc, cc;
-  first(pc);
-  cc = pc;
-  long ip = 0, ic = 0, head_p = 0, head_c = 0, tail = 0;
-  double c[4], acc[4];
-  const int tx = tid & 31, ty = tid >> 5;  // outputs (4*ty + i, tx)
+  DCursor cur, nxt;
+  if (!first(cur)) return;
+  nxt = cur;
+  bool have_next = advance(nxt);
+  load(cur, 0);
+  cp_commit();
 
-  while (cc.valid) {
-    // ---- produce: stage items ahead while slots and ring space allow ----
-    while (pc.valid && ip < ic + RG_Q) {
-      const RgItem it = item_of(pc);
-      long h = head_p;
-      const int off = place(h, it.bytes);
-      if (h - tail > RG_RING) break;  // no room until the consumer releases
-      head_p = h;
-      const uint32_t base = (uint32_t)__cvta_generic_to_shared(rsm + off);
-      const int na = it.mcnt * it.kcnt, nb = it.kcnt * it.ncnt;
-      for (int e = tid; e < na; e += RG_THREADS) {  // A piece as [m][k]
-        const int m = e / it.kcnt, k = e - m * it.kcnt;
-        cp_async8(base + e * 8, it.A + (long)(it.m0 + m) * it.lda + it.k0 + k);
-      }
-      for (int e = tid; e < nb; e += RG_THREADS) {  // op(B) piece as [k][n]
-        int k, n;
-        const double *src;
-        if (!it.transb) {
-          k = e / it.ncnt; n = e - k * it.ncnt;
-          src = it.B + (long)(it.k0 + k) * it.ldb + it.n0 + n;
-        } else {
-          n = e / it.kcnt; k = e - n * it.kcnt;
-          src = it.B + (long)(it.n0 + n) * it.ldb + it.k0 + k;
-        }
-        cp_async8(base + (na + k * it.ncnt + n) * 8, src);
-      }
-      asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];" ::"r"(
-                       (uint32_t)__cvta_generic_to_shared(&bars[ip % RG_Q]))
-                   : "memory");
-      ++ip;
-      advance(pc);
-    }
-
-    // ---- consume item ic ----
-    const RgItem it = item_of(cc);
-    const int off = place(head_c, it.bytes);
-    {
-      bool ok = false;
-      for (uint32_t n = 0; n < (1u << 22); ++n) {
-        if (rg_mbar_try(&bars[ic % RG_Q], (uint32_t)((ic / RG_Q) & 1))) { ok = true; break; }
-        if (n > 64) __nanosleep(64);
-      }
-      if (!ok) {
-        atomicOr(err, 1u);
-        s_abort = 1;
-      }
-    }
-    __syncthreads();
-    if (s_abort) break;
-    const unsigned f = run_first[cc.r];
+  double c[2][4], acc[2][4];
+  int buf = 0;
+  for (;;) {
+    const unsigned f = run_first[cur.r];
     const LibShalom_dgemm_entry &e0 = entries[f];
-    const LibShalom_dgemm_entry &ep = entries[f + cc.p];
+    const DJob jb = djob(entries[f + cur.p]);
+    const int tiles_n = (e0.N + DR_T - 1) / DR_T;
+    const int m0 = (cur.t / tiles_n) * DR_T, n0 = (cur.t % tiles_n) * DR_T;
+    double *Crow0 = entries[f].C + (long)(m0 + 2 * ty) * (e0.ldc > 0 ? e0.ldc : e0.N) + n0 + 4 * tx;
     const int ldc = e0.ldc > 0 ? e0.ldc : e0.N;
-    double *Ct = e0.C + (long)it.m0 * ldc + it.n0;
-    if (cc.p == 0 && cc.k == 0) {
+    if (cur.p == 0 && cur.k == 0) {
+      // new C tile: load it (the run's first beta decides whether it is read)
 #pragma unroll
-      for (int i = 0; i < 4; ++i) {
-        const int m = 4 * ty + i;
-        c[i] = (m < it.mcnt && tx < it.ncnt) ? Ct[(long)m * ldc + tx] : 0.0;
-      }
-    }
-    if (cc.k == 0) {
+      for (int i = 0; i < 2; ++i)
 #pragma unroll
-      for (int i = 0; i < 4; ++i) acc[i] = 0.0;
-    }
-    const double *As = reinterpret_cast<const double *>(rsm + off);
-    const double *Bs = As + it.mcnt * it.kcnt;
-    if (tx < it.ncnt) {
-      for (int k = 0; k < it.kcnt; ++k) {
-        const double b = Bs[k * it.ncnt + tx];
-#pragma unroll
-        for (int i = 0; i < 4; ++i) {
-          const int m = min(4 * ty + i, it.mcnt - 1);  // rows past mcnt: computed, not stored
-          acc[i] = __fma_rn(As[m * it.kcnt + k], b, acc[i]);
+        for (int j = 0; j < 4; ++j) {
+          const bool ok = m0 + 2 * ty + i < e0.M && n0 + 4 * tx + j < e0.N;
+          c[i][j] = ok ? Crow0[(long)i * ldc + j] : 0.0;
         }
-      }
     }
-    const bool product_done = cc.k + 1 >= kslices_of(ep);
+    if (cur.k == 0) {
+#pragma unroll
+      for (int i = 0; i < 2; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) acc[i][j] = 0.0;
+    }
+    // prefetch the next slab into the other buffer, then wait for this one
+    if (have_next) load(nxt, buf ^ 1);
+    cp_commit();
+    cp_wait<1>();
+    __syncthreads();
+    const double *As = stage[buf];
+    const double *Bs = stage[buf] + DR_T * DR_P;
+    const int kcnt = min(DR_T, jb.K - cur.k * DR_T);
+    for (int k = 0; k < kcnt; ++k) {
+      const double2 a = *reinterpret_cast<const double2 *>(As + k * DR_P + 2 * ty);
+      const double2 b0 = *reinterpret_cast<const double2 *>(Bs + k * DR_P + 4 * tx);
+      const double2 b1 = *reinterpret_cast<const double2 *>(Bs + k * DR_P + 4 * tx + 2);
+      const double av[2] = {a.x, a.y};
+      const double bv[4] = {b0.x, b0.y, b1.x, b1.y};
+#pragma unroll
+      for (int i = 0; i < 2; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) acc[i][j] = __fma_rn(av[i], bv[j], acc[i][j]);
+    }
+    const bool product_done = cur.k + 1 >= max(1, (jb.K + DR_T - 1) / DR_T);
     if (product_done) {
 #pragma unroll
-      for (int i = 0; i < 4; ++i) {
-        const double v = ep.alpha * acc[i];
-        c[i] = ep.beta != 0.0 ? __fma_rn(ep.beta, c[i], v) : v;
-      }
-      if (cc.p + 1 == (int)run_len[cc.r]) {
+      for (int i = 0; i < 2; ++i)
 #pragma unroll
-        for (int i = 0; i < 4; ++i) {
-          const int m = 4 * ty + i;
-          if (m < it.mcnt && tx < it.ncnt) Ct[(long)m * ldc + tx] = c[i];
+        for (int j = 0; j < 4; ++j) {
+          const double v = jb.alpha * acc[i][j];
+          c[i][j] = jb.beta != 0.0 ? __fma_rn(jb.beta, c[i][j], v) : v;
         }
+      if (cur.p + 1 == (int)run_len[cur.r]) {
+        // run complete for this tile: write it
+#pragma unroll
+        for (int i = 0; i < 2; ++i)
+#pragma unroll
+          for (int j = 0; j < 4; ++j)
+            if (m0 + 2 * ty + i < e0.M && n0 + 4 * tx + j < e0.N) Crow0[(long)i * ldc + j] = c[i][j];
       }
     }
-    __syncthreads();  // every thread is done reading the item: release it
-    tail = head_c;
-    ++ic;
-    advance(cc);
+    __syncthreads();  // everyone is done with this buffer before it is refilled
+    if (!have_next) break;
+    cur = nxt;
+    have_next = advance(nxt);
+    buf ^= 1;
   }
   cp_wait<0>();
-  __syncthreads();
 }
-
-// device status word of the bounded waits
-__device__ unsigned g_dr_err;
 
 }  // namespace
 
@@ -296,24 +245,10 @@ int run_dgemm_runs(const LibShalom_dgemm_entry *entries, long count) {
   const int pgrid = (int)std::max(1L, std::min(cdiv(count, 256), (long)st.num_sms * 8));
   k_drun_plan<<<pgrid, 256, 0, st.stream>>>(entries, count, pl);
   LS_CUDA_TRY(cudaGetLastError());
-  void *errp = nullptr;
-  LS_CUDA_TRY(cudaGetSymbolAddress(&errp, g_dr_err));
-  const int per_sm = std::min(2, occupancy_of((const void *)k_dgemm_ring, RG_THREADS, RG_SMEM, 1));
-  const int grid = grid_for(count, per_sm);
-  k_dgemm_ring<<<grid, RG_THREADS, RG_SMEM, st.stream>>>(entries, pl.n_runs, pl.run_first,
-                                                         pl.run_len,
-                                                         static_cast<unsigned *>(errp));
+  const int per_sm = occupancy_of((const void *)k_dgemm_runs, DR_THREADS, 0, 4);
+  const int grid = grid_for(cdiv(count, 1), per_sm);
+  k_dgemm_runs<<<grid, DR_THREADS, 0, st.stream>>>(entries, pl.n_runs, pl.run_first, pl.run_len);
   LS_CUDA_TRY(cudaGetLastError());
-  if (st.sync) {
-    unsigned err = 0;
-    LS_CUDA_TRY(cudaStreamSynchronize(st.stream));
-    LS_CUDA_TRY(cudaMemcpyFromSymbol(&err, g_dr_err, sizeof(err)));
-    if (err) {
-      const unsigned zero = 0;
-      LS_CUDA_TRY(cudaMemcpyToSymbol(g_dr_err, &zero, sizeof(zero)));
-      return LIBSHALOM_ERR_DEVICE_TIMEOUT;
-    }
-  }
   return LIBSHALOM_SUCCESS;
 }
 

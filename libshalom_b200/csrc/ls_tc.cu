@@ -241,7 +241,8 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_tc_sgemm(TcProblem p) {
 
   // ---- producer: cp.async of slab s of the producer's tile into stage st ----
   auto issue_slab = [&](long t, int s, int st) {
-    const int k0 = s * TC_BK;
+    // split-K: "GEMM" g0 of the batch is K slice g0 of one product
+    const int k0 = s * TC_BK + (p.kslice ? (int)decode_tile(p, t).g0 * p.kslice : 0);
     const uint32_t sa = smem_base + OFF_STAGE + st * STAGE_BYTES;
     const uint32_t sb = sa + STAGE_A_BYTES;
     if (p.vec_a) {
@@ -1659,7 +1660,7 @@ static int tc_pick_splits(const GemmArgs<float> &g, int forced) {
 int tc_sgemm_single(const GemmArgs<float> &g, int mode, int splits) {
   if (!tc_mode_ok(mode)) return LIBSHALOM_ERR_INVALID_VALUE;
   const int s = g.transa ? 1 : tc_pick_splits(g, splits);
-  if (s <= 1 || !state().use_tma) return tc_sgemm_strided(g, 0, 0, 0, 1, mode);
+  if (s <= 1) return tc_sgemm_strided(g, 0, 0, 0, 1, mode);
   // K slices as a batch of s partial products into the workspace, then an
   // ordered reduction C = alpha * sum_z partial_z + beta * C
   void *ws = nullptr;
@@ -1682,11 +1683,10 @@ int tc_sgemm_single(const GemmArgs<float> &g, int mode, int splits) {
   p.kslice = p.K / s;
   p.nk = p.kslice / TC_BK;
   p.kc_slabs = 128 / TC_BK;
-  p.vec_a = p.vec_b = 0;
+  // the TMA kernel when the operands allow it, else the cp.async kernel
+  p.vec_a = aligned16(g.A) && g.lda % 4 == 0;
+  p.vec_b = aligned16(g.B) && g.ldb % 4 == 0;
   p.vec_c = 1;
-  CUtensorMap ma, mb;
-  WsArgs wa;
-  if (!ws_maps(p, &ma, &mb, &wa)) return tc_sgemm_strided(g, 0, 0, 0, 1, mode);
   rc = tc_launch(p, mode);
   if (rc) return rc;
   return run_splitk_reduce_f32(partial, s, g.M, g.N, g.C, g.ldc, g.alpha, g.beta);
