@@ -972,13 +972,12 @@ struct GrpPlan {
   unsigned *n_runs;       // [1]
   unsigned *run_first;    // [count] first entry of the run in sorted slot s
   unsigned *run_len;      // [count]
-  unsigned *tile_prefix;  // [count + 1] exclusive prefix of tiles over sorted slots
 };
 
 struct GrpArgs {
   const LibShalom_sgemm_entry *entries;
   long count;
-  const unsigned *run_first, *run_len, *tile_prefix, *n_runs;
+  const unsigned *run_first, *run_len, *n_runs;
   unsigned *err;
   int kc_slabs;
 };
@@ -1003,12 +1002,6 @@ __device__ __forceinline__ int grp_run_class(const LibShalom_sgemm_entry *e, lon
   } while (j < count && e[j].C == e[i].C);
   *len = j - i;
   return (int)min(slabs, (long)GRP_CLASSES - 1);
-}
-
-__device__ __forceinline__ unsigned grp_run_tiles(const LibShalom_sgemm_entry &e) {
-  if (e.M <= 0 || e.N <= 0) return 0;
-  const int tn = grp_tile_n(e.N);
-  return (unsigned)(((e.M + TC_BM - 1) / TC_BM) * ((e.N + tn - 1) / tn));
 }
 
 // pass 1: runs per work class
@@ -1046,62 +1039,48 @@ __global__ void k_grp_place(const LibShalom_sgemm_entry *e, long count, GrpPlan 
   }
 }
 
-// pass 4 (one CTA of 1024 threads): exclusive prefix of tiles over the slots
-__global__ void __launch_bounds__(1024) k_grp_prefix(const LibShalom_sgemm_entry *e, GrpPlan pl) {
-  __shared__ unsigned warp_sums[32];
-  __shared__ unsigned carry;
-  const unsigned R = *pl.n_runs;
-  if (threadIdx.x == 0) carry = 0;
-  __syncthreads();
-  for (unsigned base = 0; base < R; base += 1024) {
-    const unsigned s = base + threadIdx.x;
-    const unsigned v = s < R ? grp_run_tiles(e[pl.run_first[s]]) : 0u;
-    unsigned x = v;  // inclusive warp scan
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-      const unsigned y = __shfl_up_sync(0xffffffffu, x, o);
-      if ((threadIdx.x & 31) >= (unsigned)o) x += y;
-    }
-    if ((threadIdx.x & 31) == 31) warp_sums[threadIdx.x >> 5] = x;
-    __syncthreads();
-    if (threadIdx.x < 32) {
-      unsigned w = warp_sums[threadIdx.x];
-#pragma unroll
-      for (int o = 1; o < 32; o <<= 1) {
-        const unsigned y = __shfl_up_sync(0xffffffffu, w, o);
-        if (threadIdx.x >= (unsigned)o) w += y;
-      }
-      warp_sums[threadIdx.x] = w;  // inclusive over warps
-    }
-    __syncthreads();
-    const unsigned warp_off = (threadIdx.x >> 5) ? warp_sums[(threadIdx.x >> 5) - 1] : 0u;
-    if (s < R) pl.tile_prefix[s] = carry + warp_off + x - v;
-    __syncthreads();
-    if (threadIdx.x == 0) carry += warp_sums[31];
-    __syncthreads();
-  }
-  if (threadIdx.x == 0) pl.tile_prefix[R] = carry;
-}
 
-// global tile index -> (run, 128-row tile, N tile)
-__device__ __forceinline__ GrpItem grp_item(const GrpArgs &g, long t) {
-  int lo = 0, hi = (int)*g.n_runs - 1;
-  while (lo < hi) {
-    const int mid = (lo + hi + 1) >> 1;
-    if ((long)g.tile_prefix[mid] <= t) lo = mid;
-    else hi = mid - 1;
+// Per-CTA walk over (run, tile): runs are taken round-robin over the CTAs in
+// the heaviest-first order of the plan, and every tile of a run is processed
+// by the CTA that takes the run.  Advancing costs two dependent loads per run.
+struct RunCursor {
+  long s;       // sorted run slot
+  int first, len, tiles, tiles_n, tn, tt;
+};
+
+__device__ __forceinline__ void run_load(const GrpArgs &g, RunCursor &rc, long n_runs) {
+  for (; rc.s < n_runs; rc.s += gridDim.x) {
+    rc.first = (int)g.run_first[rc.s];
+    rc.len = (int)g.run_len[rc.s];
+    const int M = g.entries[rc.first].M, N = g.entries[rc.first].N;
+    if (M <= 0 || N <= 0) continue;
+    rc.tn = grp_tile_n(N);
+    rc.tiles_n = (N + rc.tn - 1) / rc.tn;
+    rc.tiles = ((M + TC_BM - 1) / TC_BM) * rc.tiles_n;
+    rc.tt = 0;
+    return;
   }
+}
+__device__ __forceinline__ RunCursor run_begin(const GrpArgs &g, long n_runs) {
+  RunCursor rc;
+  rc.s = blockIdx.x;
+  run_load(g, rc, n_runs);
+  return rc;
+}
+__device__ __forceinline__ void run_next(const GrpArgs &g, RunCursor &rc, long n_runs) {
+  if (++rc.tt < rc.tiles) return;
+  rc.s += gridDim.x;
+  run_load(g, rc, n_runs);
+}
+__device__ __forceinline__ GrpItem run_item(const RunCursor &rc) {
   GrpItem it;
-  it.first = (int)g.run_first[lo];
-  it.len = (int)g.run_len[lo];
-  const int local = (int)(t - (long)g.tile_prefix[lo]);
-  const int N = g.entries[it.first].N;
-  const int tn = grp_tile_n(N);
-  const int tn_n = (N + tn - 1) / tn;
-  it.m0 = (local / tn_n) * TC_BM;
-  it.n0 = (local % tn_n) * tn;
+  it.first = rc.first;
+  it.len = rc.len;
+  it.m0 = (rc.tt / rc.tiles_n) * TC_BM;
+  it.n0 = (rc.tt % rc.tiles_n) * rc.tn;
   return it;
 }
+
 
 // one product of a work item, as every role sees it
 struct GrpJob {
@@ -1143,7 +1122,7 @@ __global__ void __launch_bounds__(G_THREADS, 1) k_tc_grouped(const GrpArgs g) {
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const uint32_t smem_base = ptx::smem_u32(smem);
   const int kc = g.kc_slabs;
-  const long n_items = (long)g.tile_prefix[*g.n_runs];
+  const long n_runs = (long)*g.n_runs;
 
   if (tid == 0) {
     for (int i = 0; i < WS_STAGES; ++i) {
@@ -1174,8 +1153,8 @@ __global__ void __launch_bounds__(G_THREADS, 1) k_tc_grouped(const GrpArgs g) {
     const int pt = tid;  // 0..63
     long j = 0;
     bool ok = true;
-    for (long t = blockIdx.x; ok && t < n_items; t += gridDim.x) {
-      const GrpItem it = grp_item(g, t);
+    for (RunCursor rc = run_begin(g, n_runs); ok && rc.s < n_runs; run_next(g, rc, n_runs)) {
+      const GrpItem it = run_item(rc);
       for (int pidx = 0; ok && pidx < it.len; ++pidx) {
         const GrpJob jb = grp_job(g, it, pidx);
         for (int s = 0; s < jb.nk; ++s, ++j) {
@@ -1251,8 +1230,8 @@ __global__ void __launch_bounds__(G_THREADS, 1) k_tc_grouped(const GrpArgs g) {
     if (lane == 0) {
       long j = 0, u = 0;
       bool ok = true;
-      for (long t = blockIdx.x; ok && t < n_items; t += gridDim.x) {
-        const GrpItem it = grp_item(g, t);
+      for (RunCursor rc = run_begin(g, n_runs); ok && rc.s < n_runs; run_next(g, rc, n_runs)) {
+        const GrpItem it = run_item(rc);
         for (int pidx = 0; ok && pidx < it.len; ++pidx) {
           const GrpJob jb = grp_job(g, it, pidx);
           const uint32_t idesc = ptx::idesc_bf16_f32(TC_BM, jb.tn);
@@ -1312,8 +1291,8 @@ __global__ void __launch_bounds__(G_THREADS, 1) k_tc_grouped(const GrpArgs g) {
     const int cr = ct & 127, cc0 = ct >> 7;
     long j = 0;
     bool ok = true;
-    for (long t = blockIdx.x; ok && t < n_items; t += gridDim.x) {
-      const GrpItem it = grp_item(g, t);
+    for (RunCursor rc = run_begin(g, n_runs); ok && rc.s < n_runs; run_next(g, rc, n_runs)) {
+      const GrpItem it = run_item(rc);
       for (int pidx = 0; ok && pidx < it.len; ++pidx) {
         const GrpJob jb = grp_job(g, it, pidx);
         const int tn = jb.tn;
@@ -1388,8 +1367,8 @@ __global__ void __launch_bounds__(G_THREADS, 1) k_tc_grouped(const GrpArgs g) {
     float R[64];
     long u = 0;
     bool ok = true;
-    for (long t = blockIdx.x; ok && t < n_items; t += gridDim.x) {
-      const GrpItem it = grp_item(g, t);
+    for (RunCursor rc = run_begin(g, n_runs); ok && rc.s < n_runs; run_next(g, rc, n_runs)) {
+      const GrpItem it = run_item(rc);
       for (int pidx = 0; ok && pidx < it.len; ++pidx) {
         const GrpJob jb = grp_job(g, it, pidx);
         const int tn = jb.tn, nch = tn / 8, per = (nch + 1) / 2;
@@ -1696,9 +1675,9 @@ int tc_sgemm_grouped(const LibShalom_sgemm_entry *entries, long count, int mode)
   if (!tc_mode_ok(mode)) return LIBSHALOM_ERR_INVALID_VALUE;
   if (count > (1L << 30)) return LIBSHALOM_ERR_UNSUPPORTED;
   State &st = state();
-  // plan workspace: 256-word header (class tables, run count), then three
+  // plan workspace: 256-word header (class tables, run count), then two
   // arrays sized by the entry count
-  const size_t words = 256 + 3 * (size_t)count + 1;
+  const size_t words = 256 + 2 * (size_t)count;
   void *ws = nullptr;
   int rc = workspace(words * sizeof(unsigned), &ws);
   if (rc) return rc;
@@ -1710,13 +1689,11 @@ int tc_sgemm_grouped(const LibShalom_sgemm_entry *entries, long count, int mode)
   pl.n_runs = w + 3 * GRP_CLASSES;
   pl.run_first = w + 256;
   pl.run_len = pl.run_first + count;
-  pl.tile_prefix = pl.run_len + count;
   LS_CUDA_TRY(cudaMemsetAsync(w, 0, 256 * sizeof(unsigned), st.stream));
   const int pgrid = (int)std::max(1L, std::min(cdiv(count, 256), (long)st.num_sms * 8));
   k_grp_count<<<pgrid, 256, 0, st.stream>>>(entries, count, pl);
   k_grp_offsets<<<1, 32, 0, st.stream>>>(pl);
   k_grp_place<<<pgrid, 256, 0, st.stream>>>(entries, count, pl);
-  k_grp_prefix<<<1, 1024, 0, st.stream>>>(entries, pl);
   LS_CUDA_TRY(cudaGetLastError());
 
   void *errp = nullptr;
@@ -1726,7 +1703,6 @@ int tc_sgemm_grouped(const LibShalom_sgemm_entry *entries, long count, int mode)
   g.count = count;
   g.run_first = pl.run_first;
   g.run_len = pl.run_len;
-  g.tile_prefix = pl.tile_prefix;
   g.n_runs = pl.n_runs;
   g.err = reinterpret_cast<unsigned *>(errp);
   g.kc_slabs = 128 / TC_BK;
