@@ -1531,8 +1531,20 @@ bool ws_maps(const TcProblem &p, CUtensorMap *ma, CUtensorMap *mb, WsArgs *wa) {
   return true;
 }
 
+// The 16-byte paths of the kernels assume 16-byte aligned rows of every GEMM
+// of the batch; a plan that claims one without it is refused on the host.
+bool vec_flags_hold(const TcProblem &p) {
+  const bool packed_cols = p.G > 1 && !p.transb && p.N % 4 != 0;
+  if (p.vec_a && !(aligned16(p.A) && p.lda % 4 == 0 && p.sA % 4 == 0)) return false;
+  if (p.vec_b && !(aligned16(p.B) && p.ldb % 4 == 0 && p.sB % 4 == 0 && !packed_cols))
+    return false;
+  if (p.vec_c && !(aligned16(p.C) && p.ldc % 4 == 0 && p.sC % 4 == 0)) return false;
+  return true;
+}
+
 int tc_launch(TcProblem &p, int mode) {
   State &st = state();
+  if (!vec_flags_hold(p)) return LIBSHALOM_ERR_UNSUPPORTED;
   void *errp = nullptr;
   LS_CUDA_TRY(cudaGetSymbolAddress(&errp, g_tc_err));
   p.err = reinterpret_cast<unsigned *>(errp);
@@ -1665,7 +1677,7 @@ int tc_sgemm_single(const GemmArgs<float> &g, int mode, int splits) {
   // the TMA kernel when the operands allow it, else the cp.async kernel
   p.vec_a = aligned16(g.A) && g.lda % 4 == 0;
   p.vec_b = aligned16(g.B) && g.ldb % 4 == 0;
-  p.vec_c = 1;
+  p.vec_c = p.N % 4 == 0;  // partials: aligned workspace, rows of N floats
   rc = tc_launch(p, mode);
   if (rc) return rc;
   return run_splitk_reduce_f32(partial, s, g.M, g.N, g.C, g.ldc, g.alpha, g.beta);
