@@ -162,7 +162,8 @@ typedef struct LibShalom_dgemm_entry {
 
 /* Grouped SGEMM over `count` entries that live in DEVICE memory.  Entries
  * are independent unless they name the same C; entries that share a C must
- * be contiguous in the array and are applied in array order by one CTA. */
+ * be contiguous in the array, have the same M and N, and are applied in
+ * array order by one CTA. */
 LIBSHALOM_API int LibShalom_sgemm_batched(const LibShalom_sgemm_entry *entries, long count);
 
 /* Uniform batch: count GEMMs of one shape, matrix g at A + g*strideA etc. */

@@ -949,19 +949,12 @@ __global__ void __launch_bounds__(WS_THREADS, 1)
 //
 // Work plan (built on the device, sized by the entry count alone, so a call
 // needs no host round trip): runs of entries sharing C are sorted by their K
-// work (counting sort over GRP_CLASSES classes, heaviest first) and a prefix
-// sum of their tile counts maps a global tile index to (run, 128-row tile,
-// N tile) by binary search.  Static round-robin over that heaviest-first order
-// balances the persistent CTAs.  The products of a run are applied in array
-// order by the one CTA that owns the tile (C = alpha_p A_p op(B_p) + beta_p C,
-// product by product).
+// work (counting sort over GRP_CLASSES classes, heaviest first) and the
+// persistent CTAs take the sorted runs round-robin.  Inside a CTA a scheduler
+// warp expands its runs into (tile, product) items for the other roles.  The
+// products of a run are applied in array order by the one CTA that owns the
+// run (C = alpha_p A_p op(B_p) + beta_p C, product by product).
 // ===========================================================================
-struct GrpItem {
-  int first;  // first entry of the run
-  int len;    // entries in the run
-  int m0, n0;
-};
-
 constexpr int GRP_CLASSES = 64;  // work classes (total K slabs of the run, capped)
 
 // workspace layout of the plan (unsigned words)
@@ -982,9 +975,6 @@ struct GrpArgs {
   int kc_slabs;
 };
 
-constexpr int G_PROD_WARPS = 2, G_W_MMA = 2, G_W_CONV0 = 3, G_W_EPI0 = 11;
-constexpr int G_WARPS = 19;
-constexpr int G_THREADS = G_WARPS * 32;
 
 __device__ __forceinline__ int grp_tile_n(int N) { return min(TC_MAX_N, (N + 15) / 16 * 16); }
 
@@ -1040,72 +1030,66 @@ __global__ void k_grp_place(const LibShalom_sgemm_entry *e, long count, GrpPlan 
 }
 
 
-// Per-CTA walk over (run, tile): runs are taken round-robin over the CTAs in
-// the heaviest-first order of the plan, and every tile of a run is processed
-// by the CTA that takes the run.  Advancing costs two dependent loads per run.
-struct RunCursor {
-  long s;       // sorted run slot
-  int first, len, tiles, tiles_n, tn, tt;
-};
-
-__device__ __forceinline__ void run_load(const GrpArgs &g, RunCursor &rc, long n_runs) {
-  for (; rc.s < n_runs; rc.s += gridDim.x) {
-    rc.first = (int)g.run_first[rc.s];
-    rc.len = (int)g.run_len[rc.s];
-    const int M = g.entries[rc.first].M, N = g.entries[rc.first].N;
-    if (M <= 0 || N <= 0) continue;
-    rc.tn = grp_tile_n(N);
-    rc.tiles_n = (N + rc.tn - 1) / rc.tn;
-    rc.tiles = ((M + TC_BM - 1) / TC_BM) * rc.tiles_n;
-    rc.tt = 0;
-    return;
-  }
-}
-__device__ __forceinline__ RunCursor run_begin(const GrpArgs &g, long n_runs) {
-  RunCursor rc;
-  rc.s = blockIdx.x;
-  run_load(g, rc, n_runs);
-  return rc;
-}
-__device__ __forceinline__ void run_next(const GrpArgs &g, RunCursor &rc, long n_runs) {
-  if (++rc.tt < rc.tiles) return;
-  rc.s += gridDim.x;
-  run_load(g, rc, n_runs);
-}
-__device__ __forceinline__ GrpItem run_item(const RunCursor &rc) {
-  GrpItem it;
-  it.first = rc.first;
-  it.len = rc.len;
-  it.m0 = (rc.tt / rc.tiles_n) * TC_BM;
-  it.n0 = (rc.tt % rc.tiles_n) * rc.tn;
-  return it;
-}
-
-
-// one product of a work item, as every role sees it
-struct GrpJob {
+// Work queue of the grouped kernel.  One scheduler warp walks the CTA's runs
+// 32 at a time (one lane per run: plan slot, run length and tile count in
+// parallel), expands them into (tile, product) items and writes the items
+// into a 32-slot ring in shared memory; the other roles read the items from
+// there.  Every item is one product on one output tile; the epilogue releases
+// its slot once the item's last accumulator has been read from TMEM, after
+// which every other role has finished with it too.
+struct __align__(16) GSlot {
   const float *A, *B;
   float *C;
-  int M, N, K, lda, ldb, ldc, transb, nk, tn;
+  int M, N, K, lda;
+  int ldbx;  // ldb, or ~ldb when B is transposed
+  int ldc, m0, n0;
   float alpha, beta;
-  bool vec_a, vec_b;
+};
+static_assert(sizeof(GSlot) == 64, "queue slot is four 16-byte words");
+
+constexpr int GQ = 32;  // queue slots
+// staging ring: the FP32 slab in the TMA kernel's layout (A and B (Trans)
+// rows of 128 bytes, 128-byte swizzle; B (NoTrans) as [32 k][tile_n])
+constexpr int G_STAGES = 4;
+constexpr int G_STAGE_A = 16384;
+constexpr int G_STAGE_BYTES = 2 * G_STAGE_A;
+constexpr int G_OFF_STAGE = 2 * BUF_BYTES;            // after the two BF16 operand buffers
+constexpr int G_OFF_BAR = G_OFF_STAGE + G_STAGES * G_STAGE_BYTES;
+constexpr int G_OFF_QBAR = G_OFF_BAR + 256;          // GQ full + GQ empty mbarriers
+constexpr int G_OFF_Q = G_OFF_QBAR + 2 * GQ * 8;    // GQ slots
+constexpr int G_SMEM = G_OFF_Q + GQ * (int)sizeof(GSlot);
+static_assert(G_SMEM <= 232448, "grouped kernel exceeds 227 KB of shared memory");
+
+// warps 0-1 producer, 2 MMA, 3 scheduler, 4-11 converters, 12-27 epilogue
+// (4 TMEM lane quarters x 4 column quarters: 32 columns of one row a thread)
+constexpr int G_PROD_WARPS = 2, G_W_MMA = 2, G_W_SCHED = 3, G_W_CONV0 = 4, G_W_EPI0 = 12;
+constexpr int G_N_EPI = 16;
+constexpr int G_WARPS = 28;
+constexpr int G_THREADS = G_WARPS * 32;
+
+// one queue item as the consuming roles use it
+struct GItem {
+  const float *A, *B;
+  float *C;
+  int M, N, K, lda, ldb, ldc, m0, n0, transb, tn, nk;
+  float alpha, beta;
 };
 
-__device__ __forceinline__ GrpJob grp_job(const GrpArgs &g, const GrpItem &it, int p) {
-  const LibShalom_sgemm_entry &e = g.entries[it.first + p];
-  GrpJob j;
-  j.A = e.A; j.B = e.B; j.C = e.C;
-  j.M = e.M; j.N = e.N; j.K = max(0, e.K);
-  j.transb = e.transb;
-  j.lda = e.lda > 0 ? e.lda : j.K;
-  j.ldb = e.ldb > 0 ? e.ldb : (e.transb ? j.K : j.N);
-  j.ldc = e.ldc > 0 ? e.ldc : j.N;
-  j.alpha = e.alpha; j.beta = e.beta;
-  j.nk = max(1, (j.K + TC_BK - 1) / TC_BK);
-  j.tn = grp_tile_n(j.N);
-  j.vec_a = (reinterpret_cast<uintptr_t>(j.A) & 15) == 0 && (j.lda & 3) == 0;
-  j.vec_b = (reinterpret_cast<uintptr_t>(j.B) & 15) == 0 && (j.ldb & 3) == 0;
-  return j;
+__device__ __forceinline__ bool q_get(const unsigned char *smem, long j, GItem &it,
+                                      volatile int *s_abort, unsigned *err) {
+  uint64_t *qfull = reinterpret_cast<uint64_t *>(const_cast<unsigned char *>(smem) + G_OFF_QBAR);
+  const int slot = (int)(j % GQ);
+  if (!ws_wait(&qfull[slot], (uint32_t)((j / GQ) & 1), s_abort, err)) return false;
+  const GSlot s = reinterpret_cast<const GSlot *>(smem + G_OFF_Q)[slot];
+  it.A = s.A; it.B = s.B; it.C = s.C;
+  it.M = s.M; it.N = s.N; it.K = s.K; it.lda = s.lda;
+  it.transb = s.ldbx < 0;
+  it.ldb = it.transb ? ~s.ldbx : s.ldbx;
+  it.ldc = s.ldc; it.m0 = s.m0; it.n0 = s.n0;
+  it.alpha = s.alpha; it.beta = s.beta;
+  it.tn = grp_tile_n(max(1, it.N));
+  it.nk = max(1, (it.K + TC_BK - 1) / TC_BK);
+  return true;
 }
 
 __device__ __forceinline__ void cp_async_mbar_arrive(uint64_t *bar) {
@@ -1113,19 +1097,54 @@ __device__ __forceinline__ void cp_async_mbar_arrive(uint64_t *bar) {
                : "memory");
 }
 
+// floats per cp.async for rows of a matrix: 4 (16-byte), 2 (8-byte) or 1
+__device__ __forceinline__ int row_vec(const float *p, int ld) {
+  const uintptr_t a = reinterpret_cast<uintptr_t>(p);
+  if ((a & 15) == 0 && (ld & 3) == 0) return 4;
+  if ((a & 7) == 0 && (ld & 1) == 0) return 2;
+  return 1;
+}
+
+__device__ __forceinline__ void cp_async8(uint32_t saddr, const void *g, int src_bytes) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"(saddr), "l"(g),
+               "r"(src_bytes)
+               : "memory");
+}
+
+// 16-byte staging chunk: n valid floats at src (0..4), the rest zero-filled;
+// vw = floats per copy the row alignment allows
+__device__ __forceinline__ void stage_chunk(uint32_t dst, const float *src, int n, int vw,
+                                            const float *any) {
+  if (vw == 4) {
+    cp_async16(dst, n > 0 ? src : any, 4 * n);
+  } else if (vw == 2) {
+    cp_async8(dst, n > 0 ? src : any, 4 * min(2, n));
+    cp_async8(dst + 8, n > 2 ? src + 2 : any, 4 * max(0, n - 2));
+  } else {
+#pragma unroll
+    for (int w = 0; w < 4; ++w) cp_async4(dst + 4 * w, w < n ? src + w : any, w < n ? 4 : 0);
+  }
+}
+
+// Rows of an item that only touch output rows / columns outside C are not
+// staged or converted: the tensor core then reads whatever an earlier item
+// left in those shared-memory rows, which reaches only output rows >= M or
+// columns >= N, never stored.  Inside the valid rows every k >= K is zero in
+// both operands, so the padded K adds exact zeros.
 template <int NSPLIT>
 __global__ void __launch_bounds__(G_THREADS, 1) k_tc_grouped(const GrpArgs g) {
   extern __shared__ __align__(1024) unsigned char smem[];
-  uint64_t *bars = reinterpret_cast<uint64_t *>(smem + WS_OFF_BAR);
-  uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(smem + WS_OFF_BAR + 8 * B_COUNT);
-  volatile int *s_abort = reinterpret_cast<volatile int *>(smem + WS_OFF_BAR + 8 * B_COUNT + 4);
+  uint64_t *bars = reinterpret_cast<uint64_t *>(smem + G_OFF_BAR);
+  uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(smem + G_OFF_BAR + 8 * B_COUNT);
+  volatile int *s_abort = reinterpret_cast<volatile int *>(smem + G_OFF_BAR + 8 * B_COUNT + 4);
+  uint64_t *qfull = reinterpret_cast<uint64_t *>(smem + G_OFF_QBAR);
+  uint64_t *qempty = qfull + GQ;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const uint32_t smem_base = ptx::smem_u32(smem);
   const int kc = g.kc_slabs;
-  const long n_runs = (long)*g.n_runs;
 
   if (tid == 0) {
-    for (int i = 0; i < WS_STAGES; ++i) {
+    for (int i = 0; i < G_STAGES; ++i) {
       ptx::mbar_init(&bars[B_FULL + i], G_PROD_WARPS * 32);
       ptx::mbar_init(&bars[B_EMPTY + i], N_CONV);
     }
@@ -1133,9 +1152,13 @@ __global__ void __launch_bounds__(G_THREADS, 1) k_tc_grouped(const GrpArgs g) {
       ptx::mbar_init(&bars[B_BFULL + i], N_CONV);
       ptx::mbar_init(&bars[B_BEMPTY + i], 1);
       ptx::mbar_init(&bars[B_AFULL + i], 1);
-      ptx::mbar_init(&bars[B_AEMPTY + i], N_EPI);
+      ptx::mbar_init(&bars[B_AEMPTY + i], G_N_EPI);
     }
     ptx::mbar_init(&bars[B_FINAL], 1);
+    for (int i = 0; i < GQ; ++i) {
+      ptx::mbar_init(&qfull[i], 1);
+      ptx::mbar_init(&qempty[i], G_N_EPI);
+    }
     *s_abort = 0;
     ptx::fence_mbar_init();
   }
@@ -1148,137 +1171,188 @@ __global__ void __launch_bounds__(G_THREADS, 1) k_tc_grouped(const GrpArgs g) {
   ptx::tc_fence_after();
   const uint32_t tmem = *tmem_slot;
 
-  if (warp < G_PROD_WARPS) {
+  if (warp == G_W_SCHED) {
+    // ------------------------------ scheduler ------------------------------
+    const long n_runs = (long)*g.n_runs;
+    const long stride = gridDim.x;
+    const unsigned FULL = 0xffffffffu;
+    GSlot *qs = reinterpret_cast<GSlot *>(smem + G_OFF_Q);
+    long q = 0;  // items written
+    bool ok = true;
+    for (long s0 = blockIdx.x; ok && s0 < n_runs; s0 += 32 * stride) {
+      const long my_s = s0 + (long)lane * stride;
+      int first = 0, len = 1, tn = 16, tiles_n = 1;
+      long items = 0;
+      if (my_s < n_runs) {
+        first = (int)g.run_first[my_s];
+        len = max(1, (int)g.run_len[my_s]);
+        const int M = g.entries[first].M, N = g.entries[first].N;
+        if (M > 0 && N > 0) {
+          tn = grp_tile_n(N);
+          tiles_n = (N + tn - 1) / tn;
+          items = (long)((M + TC_BM - 1) / TC_BM) * tiles_n * len;
+        }
+      }
+      long incl = items;  // inclusive prefix of items over the lanes
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const long y = __shfl_up_sync(FULL, incl, o);
+        if (lane >= o) incl += y;
+      }
+      const long total = __shfl_sync(FULL, incl, 31);
+      for (long base = 0; ok && base < total; base += 32) {
+        const long i = base + lane;
+        int r = 0;  // run of item i: runs whose inclusive prefix is <= i
+        for (int k = 0; k < 32; ++k) r += __shfl_sync(FULL, incl, k) <= i ? 1 : 0;
+        r = min(r, 31);
+        const long r_start = __shfl_sync(FULL, incl, r) - __shfl_sync(FULL, items, r);
+        const int r_first = __shfl_sync(FULL, first, r), r_len = __shfl_sync(FULL, len, r);
+        const int r_tn = __shfl_sync(FULL, tn, r), r_tiles_n = __shfl_sync(FULL, tiles_n, r);
+        bool lane_ok = true;
+        if (i < total) {
+          // items of a run: tile-major, products of a tile in array order
+          const long loc = i - r_start;
+          const int t = (int)(loc / r_len), p = (int)(loc - (long)t * r_len);
+          const LibShalom_sgemm_entry e = g.entries[r_first + p];
+          GSlot sl;
+          const int K = max(0, e.K);
+          sl.A = e.A; sl.B = e.B; sl.C = e.C;
+          sl.M = e.M; sl.N = e.N; sl.K = K;
+          sl.lda = e.lda > 0 ? e.lda : K;
+          const int ldb = e.ldb > 0 ? e.ldb : (e.transb ? K : e.N);
+          sl.ldbx = e.transb ? ~ldb : ldb;
+          sl.ldc = e.ldc > 0 ? e.ldc : e.N;
+          sl.m0 = (t / r_tiles_n) * TC_BM;
+          sl.n0 = (t % r_tiles_n) * r_tn;
+          sl.alpha = e.alpha; sl.beta = e.beta;
+          const long qi = q + lane;
+          const int slot = (int)(qi % GQ);
+          if (qi >= GQ &&
+              !ws_wait(&qempty[slot], (uint32_t)(((qi / GQ) - 1) & 1), s_abort, g.err)) {
+            lane_ok = false;
+          } else {
+            qs[slot] = sl;
+            mbar_arrive(&qfull[slot]);
+          }
+        }
+        ok = __all_sync(FULL, lane_ok);
+        q += min(32L, total - base);
+      }
+    }
+    if (ok && lane == 0) {
+      // end of the CTA's work: an item with M = -1
+      const int slot = (int)(q % GQ);
+      if (q < GQ || ws_wait(&qempty[slot], (uint32_t)(((q / GQ) - 1) & 1), s_abort, g.err)) {
+        GSlot sl{};
+        sl.M = -1;
+        qs[slot] = sl;
+        mbar_arrive(&qfull[slot]);
+      }
+    }
+  } else if (warp < G_PROD_WARPS) {
     // ------------------------- producer (cp.async) -------------------------
     const int pt = tid;  // 0..63
-    long j = 0;
+    constexpr int NP = G_PROD_WARPS * 32;
+    long js = 0;
     bool ok = true;
-    for (RunCursor rc = run_begin(g, n_runs); ok && rc.s < n_runs; run_next(g, rc, n_runs)) {
-      const GrpItem it = run_item(rc);
-      for (int pidx = 0; ok && pidx < it.len; ++pidx) {
-        const GrpJob jb = grp_job(g, it, pidx);
-        for (int s = 0; s < jb.nk; ++s, ++j) {
-          const int st = (int)(j % WS_STAGES);
-          if (j >= WS_STAGES &&
-              !ws_wait(&bars[B_EMPTY + st], (uint32_t)(((j / WS_STAGES) - 1) & 1), s_abort, g.err)) {
-            ok = false;
-            break;
-          }
-          const uint32_t sa = smem_base + WS_OFF_STAGE + st * WS_STAGE_BYTES;
-          const uint32_t sb = sa + 16384;
-          const int k0 = s * TC_BK;
-          // A: 128 rows x 8 chunks of 4 floats; swizzled 128-byte rows
-          for (int e = pt; e < 128 * 8; e += G_PROD_WARPS * 32) {
-            const int r = e >> 3, q = e & 7;
-            const int row = it.m0 + r, k = k0 + 4 * q;
-            const uint32_t dst = sa + r * 128 + ((q ^ (r & 7)) << 4);
-            const float *src = jb.A + (long)row * jb.lda + k;
-            if (jb.vec_a) {
-              const int n = (row < jb.M && k < jb.K) ? 4 * min(4, jb.K - k) : 0;
-              cp_async16(dst, n ? src : jb.A, n);
-            } else {
-#pragma unroll
-              for (int w = 0; w < 4; ++w) {
-                const bool v = row < jb.M && k + w < jb.K;
-                cp_async4(dst + 4 * w, v ? src + w : jb.A, v ? 4 : 0);
-              }
-            }
-          }
-          if (jb.transb) {
-            for (int e = pt; e < jb.tn * 8; e += G_PROD_WARPS * 32) {
-              const int r = e >> 3, q = e & 7;
-              const int row = it.n0 + r, k = k0 + 4 * q;
-              const uint32_t dst = sb + r * 128 + ((q ^ (r & 7)) << 4);
-              const float *src = jb.B + (long)row * jb.ldb + k;
-              if (jb.vec_b) {
-                const int n = (row < jb.N && k < jb.K) ? 4 * min(4, jb.K - k) : 0;
-                cp_async16(dst, n ? src : jb.B, n);
-              } else {
-#pragma unroll
-                for (int w = 0; w < 4; ++w) {
-                  const bool v = row < jb.N && k + w < jb.K;
-                  cp_async4(dst + 4 * w, v ? src + w : jb.B, v ? 4 : 0);
-                }
-              }
-            }
-          } else {
-            const int cpr = jb.tn >> 2;
-            for (int e = pt; e < 32 * cpr; e += G_PROD_WARPS * 32) {
-              const int kr = e / cpr, col = (e - kr * cpr) * 4;
-              const int k = k0 + kr, n = it.n0 + col;
-              const uint32_t dst = sb + (kr * jb.tn + col) * 4;
-              const float *src = jb.B + (long)k * jb.ldb + n;
-              if (jb.vec_b) {
-                const int nb = (k < jb.K && n < jb.N) ? 4 * min(4, jb.N - n) : 0;
-                cp_async16(dst, nb ? src : jb.B, nb);
-              } else {
-#pragma unroll
-                for (int w = 0; w < 4; ++w) {
-                  const bool v = k < jb.K && n + w < jb.N;
-                  cp_async4(dst + 4 * w, v ? src + w : jb.B, v ? 4 : 0);
-                }
-              }
-            }
-          }
-          cp_async_mbar_arrive(&bars[B_FULL + st]);  // arrives when this thread's copies land
+    for (long j = 0; ok; ++j) {
+      GItem it;
+      if (!q_get(smem, j, it, s_abort, g.err)) break;
+      if (it.M < 0) break;
+      const int mrows = min(TC_BM, it.M - it.m0), ncols = min(it.tn, it.N - it.n0);
+      const int va = row_vec(it.A, it.lda), vb = row_vec(it.B, it.ldb);
+      for (int s = 0; s < it.nk; ++s, ++js) {
+        const int st = (int)(js % G_STAGES);
+        if (js >= G_STAGES &&
+            !ws_wait(&bars[B_EMPTY + st], (uint32_t)(((js / G_STAGES) - 1) & 1), s_abort, g.err)) {
+          ok = false;
+          break;
         }
+        const uint32_t sa = smem_base + G_OFF_STAGE + st * G_STAGE_BYTES;
+        const uint32_t sb = sa + G_STAGE_A;
+        const int k0 = s * TC_BK;
+        const int kv = max(0, min(TC_BK, it.K - k0));  // valid k of the slab
+        // A: valid rows x 8 chunks of 4 floats; swizzled 128-byte rows
+        for (int e = pt; e < mrows * 8; e += NP) {
+          const int r = e >> 3, q = e & 7;
+          const uint32_t dst = sa + r * 128 + ((q ^ (r & 7)) << 4);
+          const float *src = it.A + (long)(it.m0 + r) * it.lda + k0 + 4 * q;
+          stage_chunk(dst, src, max(0, min(4, kv - 4 * q)), va, it.A);
+        }
+        if (it.transb) {
+          for (int e = pt; e < ncols * 8; e += NP) {
+            const int r = e >> 3, q = e & 7;
+            const uint32_t dst = sb + r * 128 + ((q ^ (r & 7)) << 4);
+            const float *src = it.B + (long)(it.n0 + r) * it.ldb + k0 + 4 * q;
+            stage_chunk(dst, src, max(0, min(4, kv - 4 * q)), vb, it.B);
+          }
+        } else {
+          // [32 k][tn] floats; the valid columns of every k row (zero past K)
+          const int cpr = (ncols + 3) >> 2;
+          for (int e = pt; e < 32 * cpr; e += NP) {
+            const int kr = e / cpr, col = (e - kr * cpr) * 4;
+            const uint32_t dst = sb + (kr * it.tn + col) * 4;
+            const float *src = it.B + (long)(k0 + kr) * it.ldb + it.n0 + col;
+            stage_chunk(dst, src, kr < kv ? min(4, ncols - col) : 0, vb, it.B);
+          }
+        }
+        cp_async_mbar_arrive(&bars[B_FULL + st]);  // arrives when this thread's copies land
       }
     }
     cp_async_wait<0>();
   } else if (warp == G_W_MMA) {
     // -------------------------------- MMA ---------------------------------
     if (lane == 0) {
-      long j = 0, u = 0;
+      long js = 0, u = 0;
       bool ok = true;
-      for (RunCursor rc = run_begin(g, n_runs); ok && rc.s < n_runs; run_next(g, rc, n_runs)) {
-        const GrpItem it = run_item(rc);
-        for (int pidx = 0; ok && pidx < it.len; ++pidx) {
-          const GrpJob jb = grp_job(g, it, pidx);
-          const uint32_t idesc = ptx::idesc_bf16_f32(TC_BM, jb.tn);
-          for (int s = 0; s < jb.nk; ++s, ++j) {
-            const int s_in = s % kc;
-            if (s_in == 0) {
-              const int a = (int)(u & 1);
-              if (u >= 2 && !ws_wait(&bars[B_AEMPTY + a], (uint32_t)(((u >> 1) - 1) & 1), s_abort,
-                                     g.err)) {
-                ok = false;
-                break;
-              }
-            }
-            const int b = (int)(j & 1);
-            if (!ws_wait(&bars[B_BFULL + b], (uint32_t)((j >> 1) & 1), s_abort, g.err)) {
+      for (long j = 0; ok; ++j) {
+        GItem it;
+        if (!q_get(smem, j, it, s_abort, g.err)) break;
+        if (it.M < 0) break;
+        const uint32_t idesc = ptx::idesc_bf16_f32(TC_BM, it.tn);
+        for (int s = 0; s < it.nk; ++s, ++js) {
+          const int s_in = s % kc;
+          if (s_in == 0) {
+            const int a = (int)(u & 1);
+            if (u >= 2 && !ws_wait(&bars[B_AEMPTY + a], (uint32_t)(((u >> 1) - 1) & 1), s_abort,
+                                   g.err)) {
               ok = false;
               break;
             }
-            ptx::tc_fence_after();
-            const uint32_t acc_base = tmem + (uint32_t)((u & 1) * 256);
-            const uint32_t bb = smem_base + WS_OFF_BUF + b * BUF_BYTES;
-            const int ksteps = max(1, min(2, (jb.K - s * TC_BK + 15) / 16));
+          }
+          const int b = (int)(js & 1);
+          if (!ws_wait(&bars[B_BFULL + b], (uint32_t)((js >> 1) & 1), s_abort, g.err)) {
+            ok = false;
+            break;
+          }
+          ptx::tc_fence_after();
+          const uint32_t acc_base = tmem + (uint32_t)((u & 1) * 256);
+          const uint32_t bb = smem_base + WS_OFF_BUF + b * BUF_BYTES;
+          const int ksteps = max(1, min(2, (it.K - s * TC_BK + 15) / 16));
 #pragma unroll
-            for (int ks = 0; ks < 2; ++ks) {
-              if (ks >= ksteps) break;
-              const uint32_t acc = (s_in > 0 || ks > 0) ? 1u : 0u;
-              uint64_t da[3], db[3];
+          for (int ks = 0; ks < 2; ++ks) {
+            if (ks >= ksteps) break;
+            const uint32_t acc = (s_in > 0 || ks > 0) ? 1u : 0u;
+            uint64_t da[3], db[3];
 #pragma unroll
-              for (int sp = 0; sp < NSPLIT; ++sp) {
-                da[sp] = ptx::smem_desc(bb + sp * SPLIT_BYTES + ks * 2 * CHUNK_BYTES, CHUNK_BYTES, 128);
-                db[sp] = ptx::smem_desc(bb + sp * SPLIT_BYTES + 8192 + ks * 2 * CHUNK_BYTES,
-                                        CHUNK_BYTES, 128);
-              }
-              ptx::mma_bf16(acc_base, da[0], db[0], idesc, acc);
-              ptx::mma_bf16(acc_base + 128, da[0], db[1], idesc, acc);
-              ptx::mma_bf16(acc_base + 128, da[1], db[0], idesc, 1u);
-              if (NSPLIT == 3) {
-                ptx::mma_bf16(acc_base + 128, da[0], db[2], idesc, 1u);
-                ptx::mma_bf16(acc_base + 128, da[2], db[0], idesc, 1u);
-                ptx::mma_bf16(acc_base + 128, da[1], db[1], idesc, 1u);
-              }
+            for (int sp = 0; sp < NSPLIT; ++sp) {
+              da[sp] = ptx::smem_desc(bb + sp * SPLIT_BYTES + ks * 2 * CHUNK_BYTES, CHUNK_BYTES, 128);
+              db[sp] = ptx::smem_desc(bb + sp * SPLIT_BYTES + 8192 + ks * 2 * CHUNK_BYTES,
+                                      CHUNK_BYTES, 128);
             }
-            ptx::mma_commit(&bars[B_BEMPTY + b]);
-            if (s_in == kc - 1 || s == jb.nk - 1) {
-              ptx::mma_commit(&bars[B_AFULL + (u & 1)]);
-              ++u;
+            ptx::mma_bf16(acc_base, da[0], db[0], idesc, acc);
+            ptx::mma_bf16(acc_base + 128, da[0], db[1], idesc, acc);
+            ptx::mma_bf16(acc_base + 128, da[1], db[0], idesc, 1u);
+            if (NSPLIT == 3) {
+              ptx::mma_bf16(acc_base + 128, da[0], db[2], idesc, 1u);
+              ptx::mma_bf16(acc_base + 128, da[2], db[0], idesc, 1u);
+              ptx::mma_bf16(acc_base + 128, da[1], db[1], idesc, 1u);
             }
+          }
+          ptx::mma_commit(&bars[B_BEMPTY + b]);
+          if (s_in == kc - 1 || s == it.nk - 1) {
+            ptx::mma_commit(&bars[B_AFULL + (u & 1)]);
+            ++u;
           }
         }
       }
@@ -1289,26 +1363,28 @@ __global__ void __launch_bounds__(G_THREADS, 1) k_tc_grouped(const GrpArgs g) {
     // ----------------------------- converters -----------------------------
     const int ct = tid - G_W_CONV0 * 32;
     const int cr = ct & 127, cc0 = ct >> 7;
-    long j = 0;
+    long js = 0;
     bool ok = true;
-    for (RunCursor rc = run_begin(g, n_runs); ok && rc.s < n_runs; run_next(g, rc, n_runs)) {
-      const GrpItem it = run_item(rc);
-      for (int pidx = 0; ok && pidx < it.len; ++pidx) {
-        const GrpJob jb = grp_job(g, it, pidx);
-        const int tn = jb.tn;
-        for (int s = 0; s < jb.nk; ++s, ++j) {
-          const int st = (int)(j % WS_STAGES), b = (int)(j & 1);
-          if (!ws_wait(&bars[B_FULL + st], (uint32_t)((j / WS_STAGES) & 1), s_abort, g.err)) {
-            ok = false;
-            break;
-          }
-          if (j >= 2 && !ws_wait(&bars[B_BEMPTY + b], (uint32_t)(((j >> 1) - 1) & 1), s_abort,
-                                 g.err)) {
-            ok = false;
-            break;
-          }
-          const unsigned char *stg = smem + WS_OFF_STAGE + st * WS_STAGE_BYTES;
-          unsigned char *base = smem + WS_OFF_BUF + b * BUF_BYTES;
+    for (long j = 0; ok; ++j) {
+      GItem it;
+      if (!q_get(smem, j, it, s_abort, g.err)) break;
+      if (it.M < 0) break;
+      const int tn = it.tn;
+      const int mrows = min(TC_BM, it.M - it.m0), ncols = min(tn, it.N - it.n0);
+      for (int s = 0; s < it.nk; ++s, ++js) {
+        const int st = (int)(js % G_STAGES), b = (int)(js & 1);
+        if (!ws_wait(&bars[B_FULL + st], (uint32_t)((js / G_STAGES) & 1), s_abort, g.err)) {
+          ok = false;
+          break;
+        }
+        if (js >= 2 && !ws_wait(&bars[B_BEMPTY + b], (uint32_t)(((js >> 1) - 1) & 1), s_abort,
+                                g.err)) {
+          ok = false;
+          break;
+        }
+        const unsigned char *stg = smem + G_OFF_STAGE + st * G_STAGE_BYTES;
+        unsigned char *base = smem + WS_OFF_BUF + b * BUF_BYTES;
+        if (cr < mrows) {
 #pragma unroll
           for (int q = 0; q < 2; ++q) {
             const int c = cc0 + 2 * q;
@@ -1324,125 +1400,129 @@ __global__ void __launch_bounds__(G_THREADS, 1) k_tc_grouped(const GrpArgs g) {
             *reinterpret_cast<uint4 *>(base + SPLIT_BYTES + off) = m;
             if (NSPLIT == 3) *reinterpret_cast<uint4 *>(base + 2 * SPLIT_BYTES + off) = l;
           }
+        }
 #pragma unroll
-          for (int q = 0; q < 2; ++q) {
-            const int e = ct + q * 256;
-            if (e < 4 * tn) {
-              const int jj = e % tn, c = e / tn;
-              float x[8];
-              if (jb.transb) {
-                const unsigned char *row = stg + 16384 + jj * 128;
-                const float4 u0 =
-                    *reinterpret_cast<const float4 *>(row + (((2 * c) ^ (jj & 7)) << 4));
-                const float4 u1 =
-                    *reinterpret_cast<const float4 *>(row + (((2 * c + 1) ^ (jj & 7)) << 4));
-                x[0] = u0.x; x[1] = u0.y; x[2] = u0.z; x[3] = u0.w;
-                x[4] = u1.x; x[5] = u1.y; x[6] = u1.z; x[7] = u1.w;
-              } else {
-                const float *fb = reinterpret_cast<const float *>(stg + 16384);
+        for (int q = 0; q < 2; ++q) {
+          const int e = ct + q * 256;
+          const int jj = e % tn, c = e / tn;
+          if (e < 4 * tn && jj < ncols) {
+            float x[8];
+            if (it.transb) {
+              const unsigned char *row = stg + G_STAGE_A + jj * 128;
+              const float4 u0 =
+                  *reinterpret_cast<const float4 *>(row + (((2 * c) ^ (jj & 7)) << 4));
+              const float4 u1 =
+                  *reinterpret_cast<const float4 *>(row + (((2 * c + 1) ^ (jj & 7)) << 4));
+              x[0] = u0.x; x[1] = u0.y; x[2] = u0.z; x[3] = u0.w;
+              x[4] = u1.x; x[5] = u1.y; x[6] = u1.z; x[7] = u1.w;
+            } else {
+              const float *fb = reinterpret_cast<const float *>(stg + G_STAGE_A);
 #pragma unroll
-                for (int tk = 0; tk < 8; ++tk) x[tk] = fb[(8 * c + tk) * tn + jj];
-              }
-              uint4 h, m, l;
-              split8<NSPLIT>(x, h, m, l);
-              const int off = 8192 + c * CHUNK_BYTES + jj * 16;
-              *reinterpret_cast<uint4 *>(base + off) = h;
-              *reinterpret_cast<uint4 *>(base + SPLIT_BYTES + off) = m;
-              if (NSPLIT == 3) *reinterpret_cast<uint4 *>(base + 2 * SPLIT_BYTES + off) = l;
+              for (int tk = 0; tk < 8; ++tk) x[tk] = fb[(8 * c + tk) * tn + jj];
             }
+            uint4 h, m, l;
+            split8<NSPLIT>(x, h, m, l);
+            const int off = 8192 + c * CHUNK_BYTES + jj * 16;
+            *reinterpret_cast<uint4 *>(base + off) = h;
+            *reinterpret_cast<uint4 *>(base + SPLIT_BYTES + off) = m;
+            if (NSPLIT == 3) *reinterpret_cast<uint4 *>(base + 2 * SPLIT_BYTES + off) = l;
           }
-          ptx::fence_proxy_async_smem();
-          __syncwarp();
-          if (lane == 0) {
-            mbar_arrive(&bars[B_EMPTY + st]);
-            mbar_arrive(&bars[B_BFULL + b]);
-          }
+        }
+        ptx::fence_proxy_async_smem();
+        __syncwarp();
+        if (lane == 0) {
+          mbar_arrive(&bars[B_EMPTY + st]);
+          mbar_arrive(&bars[B_BFULL + b]);
         }
       }
     }
   } else {
     // ------------------------------ epilogue ------------------------------
-    const int wq = warp & 3, half = (warp - G_W_EPI0) >> 2;
+    // The thread's C segment (one row, up to 32 columns) is loaded into R
+    // before the accumulator is ready, so those loads overlap the MMAs; each
+    // TMEM chunk is folded into R (the first as alpha*D + beta*C, later K
+    // chunks as R + alpha*D) and released at once; R is stored at the end.
+    const int wq = warp & 3, quarter = (warp - G_W_EPI0) >> 2;
     const int r = wq * 32 + lane;
-    float R[64];
     long u = 0;
     bool ok = true;
-    for (RunCursor rc = run_begin(g, n_runs); ok && rc.s < n_runs; run_next(g, rc, n_runs)) {
-      const GrpItem it = run_item(rc);
-      for (int pidx = 0; ok && pidx < it.len; ++pidx) {
-        const GrpJob jb = grp_job(g, it, pidx);
-        const int tn = jb.tn, nch = tn / 8, per = (nch + 1) / 2;
-        const int c_begin = min(nch, half * per), c_end = min(nch, c_begin + per);
-        const int i = it.m0 + r;
-        const bool rok = i < jb.M;
-        const int jhi = min(tn, jb.N - it.n0);
-        float *crow = jb.C + (long)i * jb.ldc + it.n0;
-        const bool vec = ((reinterpret_cast<uintptr_t>(jb.C) & 15) == 0) && (jb.ldc & 3) == 0 &&
-                         (it.n0 & 3) == 0;
+    for (long j = 0; ok; ++j) {
+      GItem it;
+      if (!q_get(smem, j, it, s_abort, g.err)) break;
+      if (it.M < 0) break;
+      const int tn = it.tn, nch = tn / 8, per = (nch + 3) / 4;
+      const int c_begin = min(nch, quarter * per), c_end = min(nch, c_begin + per);
+      const int i = it.m0 + r;
+      const bool rok = i < it.M;
+      const int jhi = min(tn, it.N - it.n0);
+      float *crow = it.C + (long)i * it.ldc + it.n0;
+      const bool vec = ((reinterpret_cast<uintptr_t>(it.C) & 15) == 0) && (it.ldc & 3) == 0;
+      const bool rd = rok && it.beta != 0.0f;
+      float R[32];
 #pragma unroll
-        for (int w = 0; w < 64; ++w) R[w] = 0.0f;
-        const int nchunks = (jb.nk + kc - 1) / kc;
-        for (int cu = 0; cu < nchunks; ++cu, ++u) {
-          const int a = (int)(u & 1);
-          if (!ws_wait(&bars[B_AFULL + a], (uint32_t)((u >> 1) & 1), s_abort, g.err)) {
-            ok = false;
-            break;
-          }
-          ptx::tc_fence_after();
-          const uint32_t acc_base = tmem + ((uint32_t)(wq * 32) << 16) + (uint32_t)(a * 256);
-#pragma unroll
-          for (int q = 0; q < 8; ++q) {
-            const int ch = c_begin + q;
-            if (ch < c_end) {
-              float dm[8], dc[8];
-              ptx::tmem_ld8(acc_base + ch * 8, dm);
-              ptx::tmem_ld8(acc_base + 128 + ch * 8, dc);
-              ptx::tmem_wait_ld();
-#pragma unroll
-              for (int w = 0; w < 8; ++w) R[q * 8 + w] += dm[w] + dc[w];
-            }
-          }
-          ptx::tc_fence_before();
-          __syncwarp();
-          if (lane == 0) mbar_arrive(&bars[B_AEMPTY + a]);
-        }
-        if (!ok || !rok) continue;
-#pragma unroll
-        for (int q = 0; q < 8; ++q) {
-          const int ch = c_begin + q;
-          if (ch >= c_end) continue;
-          const int j0 = ch * 8;
-          if (j0 >= jhi) continue;
-          const float *v = R + q * 8;
+      for (int q = 0; q < 4; ++q) {
+        const int j0 = (c_begin + q) * 8;
+        if (rd && c_begin + q < c_end && j0 < jhi) {
           if (vec && j0 + 8 <= jhi) {
-            float4 o0, o1;
-            if (jb.beta != 0.0f) {
-              const float4 c0 = *reinterpret_cast<const float4 *>(crow + j0);
-              const float4 c1 = *reinterpret_cast<const float4 *>(crow + j0 + 4);
-              o0 = make_float4(__fmaf_rn(jb.beta, c0.x, jb.alpha * v[0]),
-                               __fmaf_rn(jb.beta, c0.y, jb.alpha * v[1]),
-                               __fmaf_rn(jb.beta, c0.z, jb.alpha * v[2]),
-                               __fmaf_rn(jb.beta, c0.w, jb.alpha * v[3]));
-              o1 = make_float4(__fmaf_rn(jb.beta, c1.x, jb.alpha * v[4]),
-                               __fmaf_rn(jb.beta, c1.y, jb.alpha * v[5]),
-                               __fmaf_rn(jb.beta, c1.z, jb.alpha * v[6]),
-                               __fmaf_rn(jb.beta, c1.w, jb.alpha * v[7]));
-            } else {
-              o0 = make_float4(jb.alpha * v[0], jb.alpha * v[1], jb.alpha * v[2], jb.alpha * v[3]);
-              o1 = make_float4(jb.alpha * v[4], jb.alpha * v[5], jb.alpha * v[6], jb.alpha * v[7]);
-            }
-            *reinterpret_cast<float4 *>(crow + j0) = o0;
-            *reinterpret_cast<float4 *>(crow + j0 + 4) = o1;
+            const float4 c0 = *reinterpret_cast<const float4 *>(crow + j0);
+            const float4 c1 = *reinterpret_cast<const float4 *>(crow + j0 + 4);
+            R[q * 8 + 0] = c0.x; R[q * 8 + 1] = c0.y; R[q * 8 + 2] = c0.z; R[q * 8 + 3] = c0.w;
+            R[q * 8 + 4] = c1.x; R[q * 8 + 5] = c1.y; R[q * 8 + 6] = c1.z; R[q * 8 + 7] = c1.w;
           } else {
 #pragma unroll
-            for (int w = 0; w < 8; ++w) {
-              if (j0 + w < jhi) {
-                float x = jb.alpha * v[w];
-                if (jb.beta != 0.0f) x = __fmaf_rn(jb.beta, crow[j0 + w], x);
-                crow[j0 + w] = x;
-              }
+            for (int w = 0; w < 8; ++w) R[q * 8 + w] = j0 + w < jhi ? crow[j0 + w] : 0.0f;
+          }
+        } else {
+#pragma unroll
+          for (int w = 0; w < 8; ++w) R[q * 8 + w] = 0.0f;
+        }
+      }
+      const int nchunks = (it.nk + kc - 1) / kc;
+      for (int cu = 0; cu < nchunks; ++cu, ++u) {
+        const int a = (int)(u & 1);
+        if (!ws_wait(&bars[B_AFULL + a], (uint32_t)((u >> 1) & 1), s_abort, g.err)) {
+          ok = false;
+          break;
+        }
+        ptx::tc_fence_after();
+        const uint32_t acc_base = tmem + ((uint32_t)(wq * 32) << 16) + (uint32_t)(a * 256);
+        const float cb = cu == 0 ? (rd ? it.beta : 0.0f) : 1.0f;
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          if (c_begin + q < c_end) {
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+              float dm[4], dc[4];
+              ptx::tmem_ld4(acc_base + (c_begin + q) * 8 + 4 * h, dm);
+              ptx::tmem_ld4(acc_base + 128 + (c_begin + q) * 8 + 4 * h, dc);
+              ptx::tmem_wait_ld();
+#pragma unroll
+              for (int w = 0; w < 4; ++w)
+                R[q * 8 + 4 * h + w] =
+                    __fmaf_rn(cb, R[q * 8 + 4 * h + w], it.alpha * (dm[w] + dc[w]));
             }
           }
+        }
+        ptx::tc_fence_before();
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&bars[B_AEMPTY + a]);
+      }
+      __syncwarp();
+      if (ok && lane == 0) mbar_arrive(&qempty[j % GQ]);
+      if (!ok || !rok) continue;
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const int j0 = (c_begin + q) * 8;
+        if (c_begin + q >= c_end || j0 >= jhi) continue;
+        if (vec && j0 + 8 <= jhi) {
+          *reinterpret_cast<float4 *>(crow + j0) =
+              make_float4(R[q * 8 + 0], R[q * 8 + 1], R[q * 8 + 2], R[q * 8 + 3]);
+          *reinterpret_cast<float4 *>(crow + j0 + 4) =
+              make_float4(R[q * 8 + 4], R[q * 8 + 5], R[q * 8 + 6], R[q * 8 + 7]);
+        } else {
+#pragma unroll
+          for (int w = 0; w < 8; ++w)
+            if (j0 + w < jhi) crow[j0 + w] = R[q * 8 + w];
         }
       }
     }
@@ -1720,10 +1800,10 @@ int tc_sgemm_grouped(const LibShalom_sgemm_entry *entries, long count, int mode)
   g.kc_slabs = 128 / TC_BK;
   const void *kern = mode == LIBSHALOM_PREC_BF16X6 ? (const void *)k_tc_grouped<3>
                                                    : (const void *)k_tc_grouped<2>;
-  (void)occupancy_of(kern, G_THREADS, WS_SMEM, 1);  // raises the shared-memory limit
+  (void)occupancy_of(kern, G_THREADS, G_SMEM, 1);  // raises the shared-memory limit
   const int grid = grid_for((long)st.num_sms, 1);
   void *args[] = {&g};
-  LS_CUDA_TRY(cudaLaunchKernel(kern, dim3(grid), dim3(G_THREADS), args, WS_SMEM, st.stream));
+  LS_CUDA_TRY(cudaLaunchKernel(kern, dim3(grid), dim3(G_THREADS), args, G_SMEM, st.stream));
   LS_CUDA_TRY(cudaGetLastError());
   if (st.sync) {
     unsigned err = 0;

@@ -192,6 +192,66 @@ def test_tc_grouped_unaligned_leading_dims(mode_setter):
     assert normwise_err(got, ref) <= 1e-6
 
 
+def test_tc_grouped_even_leading_dims(mode_setter):
+    """leading dimensions that are even but not multiples of 4 (8-byte copies),
+    NN and NT"""
+    import torch
+    sdt, _ = ls.entry_dtypes()
+    M, N, K = 70, 50, 90
+    lda, ldc = 94, 58
+    for tb in (0, 1):
+        ldb = 98 if tb else 54  # >= K for B[N x K], >= N for B[K x N]
+        A = orc.uniform_f32(3 + tb, M * lda).reshape(M, lda)
+        B = orc.uniform_f32(5 + tb, (N if tb else K) * ldb).reshape(N if tb else K, ldb)
+        C = np.zeros((M, ldc), np.float32)
+        dA, dB, dC = to_dev(A), to_dev(B), to_dev(C)
+        arr = np.array([(dA.data_ptr() + 8, dB.data_ptr(), dC.data_ptr(), M, N, K, tb, lda, ldb,
+                         ldc, 1.0, 0.0, 0)], sdt)
+        ls.set_precision(ls.PREC_BF16X6)
+        ls.sgemm_batched(torch.from_numpy(arr.view(np.uint8)).cuda(), 1)
+        got = to_host(dC)[:, :N]
+        Bm = B[:, :K] if tb else B[:, :N]
+        ref = orc.sgemm_f64(np.ascontiguousarray(A[:, 2:2 + K]), np.ascontiguousarray(Bm), tb)
+        assert normwise_err(got, ref) <= 1e-6, tb
+
+
+def test_tc_grouped_small_after_large_is_exact(mode_setter):
+    """a CTA that runs a full 128x128 tile with non-finite operands and then a
+    tiny GEMM: rows and columns the tiny GEMM does not stage must not reach
+    its output"""
+    import torch
+    sdt, _ = ls.entry_dtypes()
+    sms = torch.cuda.get_device_properties(0).multi_processor_count
+    big, small = (128, 128, 96), (5, 7, 3)
+    nb = sms
+    Ab = orc.uniform_f32(11, big[0] * big[2])
+    Ab[::17] = np.inf
+    Bb = orc.uniform_f32(12, big[2] * big[1])
+    Bb[::13] = np.nan
+    As = orc.uniform_f32(13, small[0] * small[2])
+    Bs = orc.uniform_f32(14, small[2] * small[1])
+    dAb, dBb, dAs, dBs = to_dev(Ab), to_dev(Bb), to_dev(As), to_dev(Bs)
+    dCb = torch.zeros(nb * big[0] * big[1], device="cuda")
+    dCs = torch.full((nb * small[0] * small[1],), float("nan"), device="cuda")
+    ent = []
+    for i in range(nb):  # heavy runs first: one per CTA, then one light run per CTA
+        ent.append((dAb.data_ptr(), dBb.data_ptr(), dCb.data_ptr() + 4 * i * big[0] * big[1],
+                    big[0], big[1], big[2], 0, 0, 0, 0, 1.0, 0.0, 0))
+    for i in range(nb):
+        ent.append((dAs.data_ptr(), dBs.data_ptr(), dCs.data_ptr() + 4 * i * small[0] * small[1],
+                    small[0], small[1], small[2], i & 1, 0, 0, 0, 1.0, 0.0, 0))
+    arr = np.array(ent, sdt)
+    ls.set_precision(ls.PREC_BF16X6)
+    ls.sgemm_batched(torch.from_numpy(arr.view(np.uint8)).cuda(), len(arr))
+    got = to_host(dCs).reshape(nb, small[0], small[1])
+    for i in range(nb):
+        tb = i & 1
+        Bm = Bs.reshape(small[1], small[2]) if tb else Bs.reshape(small[2], small[1])
+        ref = orc.sgemm_f64(As.reshape(small[0], small[2]), Bm, tb)
+        assert np.isfinite(got[i]).all(), i
+        assert normwise_err(got[i], ref) <= 1e-6, i
+
+
 @pytest.mark.parametrize("splits", [0, 3, 8])
 def test_tc_sgemm_mp_split_k(splits, mode_setter):
     """K slices of one GEMM as a batch of partial products plus an ordered
