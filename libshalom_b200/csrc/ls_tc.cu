@@ -1060,11 +1060,12 @@ constexpr int G_OFF_Q = G_OFF_QBAR + 2 * GQ * 8;    // GQ slots
 constexpr int G_SMEM = G_OFF_Q + GQ * (int)sizeof(GSlot);
 static_assert(G_SMEM <= 232448, "grouped kernel exceeds 227 KB of shared memory");
 
-// warps 0-1 producer, 2 MMA, 3 scheduler, 4-11 converters, 12-27 epilogue
-// (4 TMEM lane quarters x 4 column quarters: 32 columns of one row a thread)
-constexpr int G_PROD_WARPS = 2, G_W_MMA = 2, G_W_SCHED = 3, G_W_CONV0 = 4, G_W_EPI0 = 12;
+// warp 0 MMA, 1 scheduler, 2-9 converters (which also stage the operands),
+// 10-25 epilogue (4 TMEM lane quarters x 4 column quarters: 32 columns of one
+// row a thread)
+constexpr int G_W_MMA = 0, G_W_SCHED = 1, G_W_CONV0 = 2, G_W_EPI0 = 10;
 constexpr int G_N_EPI = 16;
-constexpr int G_WARPS = 28;
+constexpr int G_WARPS = 26;
 constexpr int G_THREADS = G_WARPS * 32;
 
 // one queue item as the consuming roles use it
@@ -1145,7 +1146,7 @@ __global__ void __launch_bounds__(G_THREADS, 1) k_tc_grouped(const GrpArgs g) {
 
   if (tid == 0) {
     for (int i = 0; i < G_STAGES; ++i) {
-      ptx::mbar_init(&bars[B_FULL + i], G_PROD_WARPS * 32);
+      ptx::mbar_init(&bars[B_FULL + i], N_CONV * 32);
       ptx::mbar_init(&bars[B_EMPTY + i], N_CONV);
     }
     for (int i = 0; i < 2; ++i) {
@@ -1249,57 +1250,6 @@ __global__ void __launch_bounds__(G_THREADS, 1) k_tc_grouped(const GrpArgs g) {
         mbar_arrive(&qfull[slot]);
       }
     }
-  } else if (warp < G_PROD_WARPS) {
-    // ------------------------- producer (cp.async) -------------------------
-    const int pt = tid;  // 0..63
-    constexpr int NP = G_PROD_WARPS * 32;
-    long js = 0;
-    bool ok = true;
-    for (long j = 0; ok; ++j) {
-      GItem it;
-      if (!q_get(smem, j, it, s_abort, g.err)) break;
-      if (it.M < 0) break;
-      const int mrows = min(TC_BM, it.M - it.m0), ncols = min(it.tn, it.N - it.n0);
-      const int va = row_vec(it.A, it.lda), vb = row_vec(it.B, it.ldb);
-      for (int s = 0; s < it.nk; ++s, ++js) {
-        const int st = (int)(js % G_STAGES);
-        if (js >= G_STAGES &&
-            !ws_wait(&bars[B_EMPTY + st], (uint32_t)(((js / G_STAGES) - 1) & 1), s_abort, g.err)) {
-          ok = false;
-          break;
-        }
-        const uint32_t sa = smem_base + G_OFF_STAGE + st * G_STAGE_BYTES;
-        const uint32_t sb = sa + G_STAGE_A;
-        const int k0 = s * TC_BK;
-        const int kv = max(0, min(TC_BK, it.K - k0));  // valid k of the slab
-        // A: valid rows x 8 chunks of 4 floats; swizzled 128-byte rows
-        for (int e = pt; e < mrows * 8; e += NP) {
-          const int r = e >> 3, q = e & 7;
-          const uint32_t dst = sa + r * 128 + ((q ^ (r & 7)) << 4);
-          const float *src = it.A + (long)(it.m0 + r) * it.lda + k0 + 4 * q;
-          stage_chunk(dst, src, max(0, min(4, kv - 4 * q)), va, it.A);
-        }
-        if (it.transb) {
-          for (int e = pt; e < ncols * 8; e += NP) {
-            const int r = e >> 3, q = e & 7;
-            const uint32_t dst = sb + r * 128 + ((q ^ (r & 7)) << 4);
-            const float *src = it.B + (long)(it.n0 + r) * it.ldb + k0 + 4 * q;
-            stage_chunk(dst, src, max(0, min(4, kv - 4 * q)), vb, it.B);
-          }
-        } else {
-          // [32 k][tn] floats; the valid columns of every k row (zero past K)
-          const int cpr = (ncols + 3) >> 2;
-          for (int e = pt; e < 32 * cpr; e += NP) {
-            const int kr = e / cpr, col = (e - kr * cpr) * 4;
-            const uint32_t dst = sb + (kr * it.tn + col) * 4;
-            const float *src = it.B + (long)(k0 + kr) * it.ldb + it.n0 + col;
-            stage_chunk(dst, src, kr < kv ? min(4, ncols - col) : 0, vb, it.B);
-          }
-        }
-        cp_async_mbar_arrive(&bars[B_FULL + st]);  // arrives when this thread's copies land
-      }
-    }
-    cp_async_wait<0>();
   } else if (warp == G_W_MMA) {
     // -------------------------------- MMA ---------------------------------
     if (lane == 0) {
@@ -1360,11 +1310,76 @@ __global__ void __launch_bounds__(G_THREADS, 1) k_tc_grouped(const GrpArgs g) {
       ptx::mbar_wait_bounded(&bars[B_FINAL], 0);
     }
   } else if (warp < G_W_EPI0) {
-    // ----------------------------- converters -----------------------------
+    // --------------------- converters (and operand loads) ---------------------
+    // The 256 converter threads also stage the operands: before converting
+    // slab js they issue the cp.async copies of slab js + G_STAGES - 1 (a
+    // second cursor over the queue), all of them arriving on that stage's
+    // mbarrier.  Only valid rows / columns are staged; k >= K inside them is
+    // zero-filled.
     const int ct = tid - G_W_CONV0 * 32;
+    constexpr int NP = N_CONV * 32;
     const int cr = ct & 127, cc0 = ct >> 7;
-    long js = 0;
     bool ok = true;
+    // load cursor
+    long jl = 0, jsl = 0;
+    int sl = 0;
+    bool have_l = false, l_end = false;
+    GItem il;
+    auto issue_next = [&]() -> bool {
+      if (l_end) return true;
+      if (!have_l) {
+        if (!q_get(smem, jl, il, s_abort, g.err)) return false;
+        if (il.M < 0) {
+          l_end = true;
+          return true;
+        }
+        have_l = true;
+        sl = 0;
+      }
+      const int st = (int)(jsl % G_STAGES);
+      if (jsl >= G_STAGES &&
+          !ws_wait(&bars[B_EMPTY + st], (uint32_t)(((jsl / G_STAGES) - 1) & 1), s_abort, g.err))
+        return false;
+      const int mrows = min(TC_BM, il.M - il.m0), ncols = min(il.tn, il.N - il.n0);
+      const int va = row_vec(il.A, il.lda), vb = row_vec(il.B, il.ldb);
+      const uint32_t sa = smem_base + G_OFF_STAGE + st * G_STAGE_BYTES;
+      const uint32_t sb = sa + G_STAGE_A;
+      const int k0 = sl * TC_BK;
+      const int kv = max(0, min(TC_BK, il.K - k0));  // valid k of the slab
+      // A: valid rows x 8 chunks of 4 floats; swizzled 128-byte rows
+      for (int e = ct; e < mrows * 8; e += NP) {
+        const int r = e >> 3, q = e & 7;
+        const uint32_t dst = sa + r * 128 + ((q ^ (r & 7)) << 4);
+        const float *src = il.A + (long)(il.m0 + r) * il.lda + k0 + 4 * q;
+        stage_chunk(dst, src, max(0, min(4, kv - 4 * q)), va, il.A);
+      }
+      if (il.transb) {
+        for (int e = ct; e < ncols * 8; e += NP) {
+          const int r = e >> 3, q = e & 7;
+          const uint32_t dst = sb + r * 128 + ((q ^ (r & 7)) << 4);
+          const float *src = il.B + (long)(il.n0 + r) * il.ldb + k0 + 4 * q;
+          stage_chunk(dst, src, max(0, min(4, kv - 4 * q)), vb, il.B);
+        }
+      } else {
+        // [32 k][tn] floats; the valid columns of every k row (zero past K)
+        const int cpr = (ncols + 3) >> 2;
+        for (int e = ct; e < 32 * cpr; e += NP) {
+          const int kr = e / cpr, col = (e - kr * cpr) * 4;
+          const uint32_t dst = sb + (kr * il.tn + col) * 4;
+          const float *src = il.B + (long)(k0 + kr) * il.ldb + il.n0 + col;
+          stage_chunk(dst, src, kr < kv ? min(4, ncols - col) : 0, vb, il.B);
+        }
+      }
+      cp_async_mbar_arrive(&bars[B_FULL + st]);  // arrives when this thread's copies land
+      ++jsl;
+      if (++sl == il.nk) {
+        have_l = false;
+        ++jl;
+      }
+      return true;
+    };
+    for (int i = 0; ok && i < G_STAGES - 1; ++i) ok = issue_next();
+    long js = 0;
     for (long j = 0; ok; ++j) {
       GItem it;
       if (!q_get(smem, j, it, s_abort, g.err)) break;
@@ -1372,6 +1387,10 @@ __global__ void __launch_bounds__(G_THREADS, 1) k_tc_grouped(const GrpArgs g) {
       const int tn = it.tn;
       const int mrows = min(TC_BM, it.M - it.m0), ncols = min(tn, it.N - it.n0);
       for (int s = 0; s < it.nk; ++s, ++js) {
+        if (!issue_next()) {
+          ok = false;
+          break;
+        }
         const int st = (int)(js % G_STAGES), b = (int)(js & 1);
         if (!ws_wait(&bars[B_FULL + st], (uint32_t)((js / G_STAGES) & 1), s_abort, g.err)) {
           ok = false;
@@ -1436,6 +1455,7 @@ __global__ void __launch_bounds__(G_THREADS, 1) k_tc_grouped(const GrpArgs g) {
         }
       }
     }
+    cp_async_wait<0>();
   } else {
     // ------------------------------ epilogue ------------------------------
     // The thread's C segment (one row, up to 32 columns) is loaded into R
