@@ -606,7 +606,40 @@ def wl_dgemm_runs(args, count=200_000, run=8):
     dE = torch.from_numpy(ent.view(np.uint8)).cuda()
     flops = float(2.0 * (M * N * K).sum())
     alg_bytes = float(8.0 * (a_len.sum() + b_len.sum() + 2 * c_len.sum()))
-    ms = _time_events(torch, s, lambda: ls.dgemm_batched(dE, count), args.steps, args.warmup)
+    # max normwise error per C block over a sample of runs, against torch FP64
+    # applied product by product on the GPU (C0 + sum of the run's products)
+    samp = rng.choice(nruns, size=min(nruns, 300), replace=False)
+
+    def run_error():
+        err = 0.0
+        for r in samp:
+            i0 = int(r) * run
+            M0, N0 = int(M[i0]), int(N[i0])
+            c = dC0[offC[i0]:offC[i0] + M0 * N0].view(M0, N0).clone()
+            for i in range(i0, i0 + run):
+                a = dA[offA[i]:offA[i] + M0 * int(K[i])].view(M0, int(K[i]))
+                bm = dB[offB[i]:offB[i] + int(K[i]) * N0].view(int(K[i]), N0)
+                c += a @ bm
+            got = dC[offC[i0]:offC[i0] + M0 * N0].view(M0, N0)
+            e = ((got - c).abs().max() / c.abs().max()).item()
+            err = e if not (e <= err) else err  # NaN propagates
+        return err
+
+    methods = {}
+    for name, meth, sl in (("fma", ls.DGEMM_FMA, 0), ("dmma", ls.DGEMM_DMMA, 0),
+                           ("ozaki9", ls.DGEMM_OZAKI, 9), ("ozaki8", ls.DGEMM_OZAKI, 8)):
+        ls.set_dgemm_method(meth, sl)
+        dC.copy_(dC0)
+        ls.dgemm_batched(dE, count)
+        s.synchronize()
+        err = run_error()
+        mms = _time_events(torch, s, lambda: ls.dgemm_batched(dE, count), args.steps, args.warmup)
+        methods[name] = {"gflops": flops / (mms / 1e3) / 1e9, "ms": mms, "max_normwise_err": err,
+                         "gbs": alg_bytes / (mms / 1e3) / 1e9}
+    ls.set_dgemm_method(ls.DGEMM_FMA, 0)
+    ok = {k: v for k, v in methods.items() if v["max_normwise_err"] <= 1e-14}
+    best = min(ok, key=lambda k: ok[k]["ms"]) if ok else "fma"
+    ms = methods[best]["ms"]
     # per-call plain FP64 kernel over a sample of the same products
     sample = 4000
     C1 = dC.clone()
@@ -622,9 +655,10 @@ def wl_dgemm_runs(args, count=200_000, run=8):
           ms, args,
           {"workload": "LibShalom_dgemm_batched, C += A B, M,N per run and K per product from "
                        "{5,9,13,16,22,23,26,32}, entries normal(0,1)*10^u, u~U[-3,3] per matrix",
-           "products": count, "run": run, "step_gflop": flops / 1e9, "step_gbytes": alg_bytes / 1e9},
+           "products": count, "run": run, "method": best,
+           "step_gflop": flops / 1e9, "step_gbytes": alg_bytes / 1e9},
           alg_bytes,
-          {"dtype": "f64", "gpu_launches": 2 * args.steps,
+          {"dtype": "f64", "gpu_launches": 3 * args.steps, "methods": methods,
            "per_call_plain_fp64": {"gflops": pc_gflops, "sample_products": sample,
                                    "note": "loop of LibShalom_dgemm (overwrite semantics) on the "
                                            "first products, stream-ordered"},

@@ -188,8 +188,24 @@ LIBSHALOM_API int LibShalom_sgemm_mp_noalloc(int transa, int transb, float *C, c
                                              const float *B, long M, long N, long K,
                                              int splits);
 
-/* Grouped DGEMM (same rules as LibShalom_sgemm_batched; FP64 FMA). */
+/* Grouped DGEMM (same rules as LibShalom_sgemm_batched).  Arithmetic set by
+ * LibShalom_set_dgemm_method. */
 LIBSHALOM_API int LibShalom_dgemm_batched(const LibShalom_dgemm_entry *entries, long count);
+
+/* Arithmetic of LibShalom_dgemm_batched (no counterpart in the reference).
+ * Runs whose C block is larger than 32 x 32 always take the FMA kernel. */
+#define LIBSHALOM_DGEMM_FMA 0   /* FP64 FMA on the CUDA cores (default) */
+#define LIBSHALOM_DGEMM_DMMA 1  /* FP64 tensor cores (mma.sync m8n8k4 f64) */
+#define LIBSHALOM_DGEMM_OZAKI 2 /* Ozaki scheme: INT8 digit slices on the tensor
+                                   cores, exact INT32 sums, FP64 recombination;
+                                   finite inputs only */
+/* slices: signed 7-bit digits per operand element for LIBSHALOM_DGEMM_OZAKI,
+ * 4..9, 0 = 9.  Each product's error is about (S + 4) 2^(-7S) K max|A_i.|
+ * max|op(B)_.j| per element: 9 digits keep it near 1e-16 of that scale, 8
+ * near 2e-15, which can exceed 1e-14 of max|C| after cancellation.  Ignored
+ * by the other methods. */
+LIBSHALOM_API int LibShalom_set_dgemm_method(int method, int slices);
+LIBSHALOM_API int LibShalom_get_dgemm_method(void);
 
 #ifdef __cplusplus
 }

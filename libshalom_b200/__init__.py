@@ -36,6 +36,9 @@ ERR_DEVICE_TIMEOUT = 6
 PREC_FP32 = 0
 PREC_BF16X3 = 1
 PREC_BF16X6 = 2
+DGEMM_FMA = 0
+DGEMM_DMMA = 1
+DGEMM_OZAKI = 2
 
 # every symbol include/LibShalom.h declares
 EXPORTED = (
@@ -44,6 +47,7 @@ EXPORTED = (
     "LibShalom_get_last_error", "LibShalom_error_string",
     "LibShalom_set_stream", "LibShalom_set_sync", "LibShalom_synchronize",
     "LibShalom_set_precision", "LibShalom_get_precision", "LibShalom_set_splitk",
+    "LibShalom_set_dgemm_method", "LibShalom_get_dgemm_method",
     "LibShalom_set_tma",
     "LibShalom_finalize",
     "LibShalom_sgemm_batched", "LibShalom_sgemm_batched_strided",
@@ -91,6 +95,8 @@ _SIGS = {
     "LibShalom_synchronize": (_I, []),
     "LibShalom_set_precision": (_I, [_I]),
     "LibShalom_get_precision": (_I, []),
+    "LibShalom_set_dgemm_method": (_I, [_I, _I]),
+    "LibShalom_get_dgemm_method": (_I, []),
     "LibShalom_set_splitk": (_I, [_I]),
     "LibShalom_set_tma": (_I, [_I]),
     "LibShalom_finalize": (None, []),
@@ -209,6 +215,17 @@ def set_precision(mode: int) -> None:
 
 def get_precision() -> int:
     return lib().LibShalom_get_precision()
+
+
+def set_dgemm_method(method: int, slices: int = 0) -> None:
+    """Arithmetic of dgemm_batched: DGEMM_FMA, DGEMM_DMMA or DGEMM_OZAKI
+    (slices: INT8 digits per operand element, 4..9, 0 = 9)."""
+    _check(lib().LibShalom_set_dgemm_method(int(method), int(slices)),
+           "LibShalom_set_dgemm_method")
+
+
+def get_dgemm_method() -> int:
+    return lib().LibShalom_get_dgemm_method()
 
 
 def set_splitk(splits: int) -> None:

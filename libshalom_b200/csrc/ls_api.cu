@@ -261,6 +261,24 @@ int LibShalom_set_precision(int mode) {
 
 int LibShalom_get_precision(void) { return state().precision; }
 
+int LibShalom_set_dgemm_method(int method, int slices) {
+  std::lock_guard<std::mutex> lk(state().mu);
+  int rc = LIBSHALOM_SUCCESS;
+  if (method != LIBSHALOM_DGEMM_FMA && method != LIBSHALOM_DGEMM_DMMA &&
+      method != LIBSHALOM_DGEMM_OZAKI)
+    rc = LIBSHALOM_ERR_INVALID_VALUE;
+  else if (slices != 0 && (slices < 4 || slices > 9))
+    rc = LIBSHALOM_ERR_INVALID_VALUE;
+  else {
+    state().dgemm_method = method;
+    state().ozaki_slices = slices == 0 ? 9 : slices;
+  }
+  set_error(rc);
+  return rc;
+}
+
+int LibShalom_get_dgemm_method(void) { return state().dgemm_method; }
+
 int LibShalom_set_splitk(int splits) {
   std::lock_guard<std::mutex> lk(state().mu);
   int rc = LIBSHALOM_SUCCESS;
@@ -339,7 +357,10 @@ int LibShalom_dgemm_batched(const LibShalom_dgemm_entry *entries, long count) {
   int rc = LIBSHALOM_SUCCESS;
   if (!entries_ok(entries, count)) rc = LIBSHALOM_ERR_INVALID_VALUE;
   else if (count > 0 && !(rc = ensure_device())) {
-    rc = run_grouped_d(entries, count);
+    const State &st = state();
+    rc = st.dgemm_method == LIBSHALOM_DGEMM_FMA
+             ? run_grouped_d(entries, count)
+             : run_dgemm_warp(entries, count, st.dgemm_method, st.ozaki_slices);
     if (!rc) rc = finish_launch("dgemm_batched");
   }
   set_error(rc);

@@ -44,6 +44,8 @@ struct State {
   int thread_cap = 0;        // LibShalom_set_thread_nums; <=0 = no cap
   int ways_m = 0, ways_n = 0;  // LibShalom_set_thread_ways (one-shot)
   int precision = LIBSHALOM_PREC_FP32;
+  int dgemm_method = LIBSHALOM_DGEMM_FMA;
+  int ozaki_slices = 9;
   int splitk = 0;
   // tensor-core kernels: the TMA warp-specialized variant where the operands
   // allow it (LIBSHALOM_NO_TMA=1 in the environment selects the cp.async one)

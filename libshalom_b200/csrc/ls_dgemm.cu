@@ -252,4 +252,15 @@ int run_dgemm_runs(const LibShalom_dgemm_entry *entries, long count) {
   return LIBSHALOM_SUCCESS;
 }
 
+// The run kernel over a run list built by another plan (device counts).
+int run_dgemm_runs_list(const LibShalom_dgemm_entry *entries, long count, const unsigned *n_runs,
+                        const unsigned *run_first, const unsigned *run_len) {
+  State &st = state();
+  const int per_sm = occupancy_of((const void *)k_dgemm_runs, DR_THREADS, 0, 4);
+  const int grid = grid_for(cdiv(count, 1), per_sm);
+  k_dgemm_runs<<<grid, DR_THREADS, 0, st.stream>>>(entries, n_runs, run_first, run_len);
+  LS_CUDA_TRY(cudaGetLastError());
+  return LIBSHALOM_SUCCESS;
+}
+
 }  // namespace ls

@@ -33,6 +33,11 @@ int run_splitk_reduce_f32(const float *partial, int splits, long M, long N, floa
                           float alpha, float beta);
 // ls_dgemm.cu: runs of products sharing C, C tile held in registers
 int run_dgemm_runs(const LibShalom_dgemm_entry *entries, long count);
+int run_dgemm_runs_list(const LibShalom_dgemm_entry *entries, long count, const unsigned *n_runs,
+                        const unsigned *run_first, const unsigned *run_len);
+// ls_dgemm_warp.cu: runs with M, N <= 32 on the FP64 (DMMA) or INT8 (Ozaki)
+// tensor cores, the rest through run_dgemm_runs_list
+int run_dgemm_warp(const LibShalom_dgemm_entry *entries, long count, int method, int slices);
 
 // Plain FP32 split-K GEMM (GEMM_K-aligned slices, rounding order of the mp
 // path per slice) with the partial sums in `partial` (>= splits * M * N
