@@ -8,14 +8,17 @@
 // and the result does not depend on scheduling.  Runs with M or N > 32 go to
 // the CUDA-core tile kernel.
 //
-// Operand staging: every product is cut into K pieces of at most 32; for a
-// piece the warp copies each row segment of A and op(B) (and, once per run, of
-// C) as the 16-byte aligned window around it (cp.async 16 B, any leading
-// dimension, any 8-byte alignment) into one of three per-warp slots, two
-// pieces ahead of the one it multiplies.  A row's data starts 0 or 1 doubles
-// into its window (its address mod 16).  The description of every piece goes
-// into a per-warp ring next to the slots, so the entries, run table and
-// pointer arithmetic stay on the load side.
+// Operand staging: every product is cut into K pieces (at most 32, fewer when
+// A and op(B) of 32 would not fit a slot), and the warp copies each piece into
+// one of three 8.5 KB per-warp slots, two pieces ahead of the one it
+// multiplies, with 16-byte cp.async only (any leading dimension, any 8-byte
+// alignment): an operand whose piece is one contiguous range (leading
+// dimension equal to the row length) is copied as the 16-byte aligned window
+// around that range; otherwise every row segment is copied as its own window
+// at a pitch of 16 (len/2 + 1) bytes.  Data starts 0 or 1 doubles into a
+// window (the address mod 16).  The description of every piece goes into a
+// per-warp ring next to the slots, so the entries, run table and pointer
+// arithmetic stay on the load side.
 //
 // Arithmetic:
 //   DMMA   mma.sync m8n8k4 FP64 (the FP64 tensor-core instruction; tcgen05 has
@@ -40,11 +43,9 @@ namespace ls {
 
 namespace {
 
-constexpr int DW_WARPS = 4;                // warps per CTA (one run each)
+constexpr int DW_WARPS = 8;                // warps per CTA (one run each)
 constexpr int DW_SLOTS = 3;                // staging slots per warp
-constexpr int DW_PITCH = 272;              // bytes per staged row: 17 x 16 B window
-constexpr int DW_HALF = 32 * DW_PITCH;     // 32 rows (A or C | op(B) rows)
-constexpr int DW_SLOT_BYTES = 2 * DW_HALF; // 17408
+constexpr int DW_SLOT_BYTES = 8704;        // a 32 x 32 C block as row windows (32 x 272 B)
 constexpr int DW_MAXK = 32;                // K per piece
 
 enum : int { PF_FIRST_OF_PRODUCT = 1, PF_LOAD_C = 2, PF_LAST_OF_RUN = 4 };
@@ -55,6 +56,10 @@ struct __align__(16) DPiece {
   double *C;
   double alpha, beta;
   int M, N, kc, lda, ldb, ldc, transb, flags;
+  // staged layout of A (or of C in the C piece) and of B: B's byte offset in
+  // the slot, and per operand flat (one window) or row windows, the distance
+  // in doubles between row starts, and the source address's double parity
+  int b_off, a_flat, a_step, a_sh0, b_flat, b_step, b_sh0, pad_;
 };
 constexpr int DW_WARP_BYTES = DW_SLOTS * DW_SLOT_BYTES + DW_SLOTS * (int)sizeof(DPiece);
 constexpr int DW_SMEM = DW_WARPS * DW_WARP_BYTES;
@@ -94,28 +99,60 @@ __device__ __forceinline__ void cp_wait() {
   asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
 }
 
-// stage `rows` row segments of `len` doubles (row r at p + r*ld) into
-// dst + r*DW_PITCH as their 16-byte windows (only 16-byte blocks that hold
-// at least one element of the segment are read)
-__device__ __forceinline__ void stage_rows(uint32_t dst, const double *p, int rows, int len, int ld,
-                                           int lane) {
-  if (rows <= 0 || len <= 0) return;
-  for (int e = lane; e < rows * 17; e += 32) {
-    const int r = e / 17, q = e - r * 17;
+// Staged matrix of `rows` row segments of `len` doubles (row r at p + r*ld).
+// Bytes a layout takes in a slot:
+//   flat (one window over the whole range, for ld == len or a single row)
+//   rows (one window per row at a pitch of 16 (len/2 + 1) bytes)
+__device__ __forceinline__ bool can_flat(int rows, int len, int ld) { return ld == len || rows == 1; }
+__device__ __forceinline__ int flat_bytes(int rows, int len, int ld) {
+  return 16 * ((8 * ((rows - 1) * ld + len) + 8 + 15) / 16);
+}
+__device__ __forceinline__ int win_pitch(int len) { return 16 * (len / 2 + 1); }
+__device__ __forceinline__ int stage_bytes(int rows, int len, int ld) {
+  if (rows <= 0 || len <= 0) return 0;
+  return can_flat(rows, len, ld) ? flat_bytes(rows, len, ld) : rows * win_pitch(len);
+}
+
+// copy the staged matrix into dst with 16-byte cp.async (only 16-byte blocks
+// that hold at least one element are read); returns the layout fields
+__device__ __forceinline__ void stage_mat(uint32_t dst, const double *p, int rows, int len, int ld,
+                                      int lane, int &flat, int &step, int &sh0) {
+  const uintptr_t a0 = reinterpret_cast<uintptr_t>(p);
+  sh0 = (int)((a0 >> 3) & 1);
+  if (rows <= 0 || len <= 0) {
+    flat = 1; step = ld;
+    return;
+  }
+  if (can_flat(rows, len, ld)) {
+    flat = 1; step = ld;
+    const uintptr_t w0 = a0 & ~uintptr_t(15);
+    const uintptr_t end = a0 + 8 * ((uintptr_t)(rows - 1) * ld + len);
+    const int chunks = (int)((end - w0 + 15) >> 4);
+    for (int q = lane; q < chunks; q += 32) cp16(dst + 16 * q, w0 + 16 * q);
+    return;
+  }
+  flat = 0;
+  const int cpr = len / 2 + 1, pitch = 16 * cpr;
+  step = pitch / 8;
+  const int per = 32 / cpr, lr = lane / cpr, lq = lane - lr * cpr;
+  if (lr >= per) return;
+  for (int r = lr; r < rows; r += per) {
     const uintptr_t a = reinterpret_cast<uintptr_t>(p + (long)r * ld);
-    const uintptr_t w = (a & ~uintptr_t(15)) + 16 * q;
-    if (w < a + 8 * (uintptr_t)len) cp16(dst + r * DW_PITCH + 16 * q, w);
+    const uintptr_t w = (a & ~uintptr_t(15)) + 16 * lq;
+    if (w < a + 8 * (uintptr_t)len) cp16(dst + r * pitch + 16 * lq, w);
   }
 }
 
-// first element of staged row r: 0 or 1 doubles into the window
-__device__ __forceinline__ int row_shift(const double *p, int r, int ld) {
-  return (int)(((uint32_t)(reinterpret_cast<uintptr_t>(p) >> 3) + (uint32_t)r * (uint32_t)ld) & 1u);
-}
-
-__device__ __forceinline__ double lds64(const unsigned char *base, int r, int sh, int c) {
-  return *reinterpret_cast<const double *>(base + r * DW_PITCH + (sh + c) * 8);
-}
+// a staged matrix as the compute side reads it
+struct SView {
+  const double *base;
+  int flat, step, sh0, ld;
+  // double index of row r's first element
+  __device__ __forceinline__ int start(int r) const {
+    return flat ? sh0 + r * ld : r * step + ((sh0 + r * ld) & 1);
+  }
+  __device__ __forceinline__ double at(int r, int c) const { return base[start(r) + c]; }
+};
 
 // entry fields a lane holds for one product of the current run
 struct DEnt {
@@ -187,7 +224,8 @@ struct DLoader {
       pc.flags = PF_LOAD_C;
       pc.A = nullptr; pc.B = nullptr; pc.kc = 0; pc.lda = pc.ldb = 0; pc.transb = 0;
       pc.alpha = 1.0; pc.beta = 1.0;
-      stage_rows(sa, C, M, N, ldc, lane);
+      pc.b_off = 0; pc.b_flat = 1; pc.b_step = 0; pc.b_sh0 = 0;
+      stage_mat(sa, C, M, N, ldc, lane, pc.a_flat, pc.a_step, pc.a_sh0);
       stage = 1;
     } else {
       const int src = p - base;
@@ -203,18 +241,27 @@ struct DLoader {
       e.transb = __shfl_sync(FULL, ent.transb, src);
       e.alpha = __shfl_sync(FULL, ent.alpha, src);
       e.beta = __shfl_sync(FULL, ent.beta, src);
-      const int kc = min(DW_MAXK, e.K - kc0);
+      // the longest piece (<= 32) whose A and op(B) fit a slot
+      int kc = max(0, min(DW_MAXK, e.K - kc0));
+      auto bytes_of = [&](int k) {
+        const int ba = (stage_bytes(M, k, e.lda) + 15) & ~15;
+        return ba + (e.transb ? stage_bytes(N, k, e.ldb) : stage_bytes(k, N, e.ldb));
+      };
+      while (kc > 1 && bytes_of(kc) > DW_SLOT_BYTES) kc = kc > 4 ? (kc - 1) & ~3 : kc - 1;
       pc.flags = kc0 == 0 ? PF_FIRST_OF_PRODUCT : 0;
       pc.A = e.A + kc0;
       pc.B = e.transb ? e.B + kc0 : e.B + (long)kc0 * e.ldb;
-      pc.kc = max(0, kc);
+      pc.kc = kc;
       pc.lda = e.lda; pc.ldb = e.ldb; pc.transb = e.transb;
       pc.alpha = e.alpha; pc.beta = e.beta;
-      stage_rows(sa, pc.A, M, pc.kc, pc.lda, lane);
-      if (e.transb) stage_rows(sa + DW_HALF, pc.B, N, pc.kc, pc.ldb, lane);
-      else stage_rows(sa + DW_HALF, pc.B, pc.kc, N, pc.ldb, lane);
-      // advance
-      kc0 += DW_MAXK;
+      pc.b_off = (stage_bytes(M, kc, e.lda) + 15) & ~15;
+      stage_mat(sa, pc.A, M, kc, pc.lda, lane, pc.a_flat, pc.a_step, pc.a_sh0);
+      if (e.transb)
+        stage_mat(sa + pc.b_off, pc.B, N, kc, pc.ldb, lane, pc.b_flat, pc.b_step, pc.b_sh0);
+      else
+        stage_mat(sa + pc.b_off, pc.B, kc, N, pc.ldb, lane, pc.b_flat, pc.b_step, pc.b_sh0);
+      // advance (a product with K = 0 is one empty piece)
+      kc0 += max(kc, 1);
       if (kc0 >= e.K) {
         kc0 = 0;
         if (++p >= len) {
@@ -249,30 +296,30 @@ struct ArithDmma {
     row = 8 * mf + (lane >> 2);
     col = 8 * nf + 2 * (lane & 3) + h;
   }
-  __device__ static void piece(double (&acc)[32], const DPiece &pc, const unsigned char *sA,
-                               const unsigned char *sB, int lane) {
+  __device__ static void piece(double (&acc)[32], const DPiece &pc, const SView &A,
+                               const SView &B, int lane) {
     const int gr = lane >> 2, gc = lane & 3;
     const int MF = (pc.M + 7) >> 3, NF = (pc.N + 7) >> 3;
-    int shA[4], shB[4];
+    int sa[4], sb[4];  // row starts this thread reads
 #pragma unroll
     for (int mf = 0; mf < 4; ++mf) {
       const int rr = 8 * mf + gr;
-      shA[mf] = rr < pc.M ? row_shift(pc.A, rr, pc.lda) : 0;
+      sa[mf] = rr < pc.M ? A.start(rr) : 0;
     }
 #pragma unroll
     for (int nf = 0; nf < 4; ++nf) {
       const int nn = 8 * nf + gr;
-      shB[nf] = pc.transb && nn < pc.N ? row_shift(pc.B, nn, pc.ldb) : 0;
+      sb[nf] = pc.transb && nn < pc.N ? B.start(nn) : 0;
     }
     const bool scale = pc.alpha != 1.0;
     for (int k0 = 0; k0 < pc.kc; k0 += 4) {
       const int k = k0 + gc;
-      const int shk = (!pc.transb && k < pc.kc) ? row_shift(pc.B, k, pc.ldb) : 0;
+      const int skb = (!pc.transb && k < pc.kc) ? B.start(k) : 0;
       double a[4], b[4];
 #pragma unroll
       for (int mf = 0; mf < 4; ++mf) {
         const int rr = 8 * mf + gr;
-        a[mf] = (mf < MF && rr < pc.M && k < pc.kc) ? lds64(sA, rr, shA[mf], k) : 0.0;
+        a[mf] = (mf < MF && rr < pc.M && k < pc.kc) ? A.base[sa[mf] + k] : 0.0;
         if (scale) a[mf] *= pc.alpha;
       }
 #pragma unroll
@@ -280,7 +327,7 @@ struct ArithDmma {
         const int nn = 8 * nf + gr;
         double v = 0.0;
         if (nf < NF && nn < pc.N && k < pc.kc)
-          v = pc.transb ? lds64(sB, nn, shB[nf], k) : lds64(sB, k, shk, nn);
+          v = pc.transb ? B.base[sb[nf] + k] : B.base[skb + nn];
         b[nf] = v;
       }
 #pragma unroll
@@ -348,25 +395,24 @@ struct ArithOzaki {
     row = 16 * mt + (lane >> 2) + 8 * (q >> 1);
     col = 8 * nt + 2 * (lane & 3) + (q & 1);
   }
-  __device__ static double opb(const DPiece &pc, const unsigned char *sB, int k, int n) {
-    return pc.transb ? lds64(sB, n, row_shift(pc.B, n, pc.ldb), k)
-                     : lds64(sB, k, row_shift(pc.B, k, pc.ldb), n);
+  __device__ static double opb(const DPiece &pc, const SView &B, int k, int n) {
+    return pc.transb ? B.at(n, k) : B.at(k, n);
   }
-  __device__ static void piece(double (&acc)[32], const DPiece &pc, const unsigned char *sA,
-                               const unsigned char *sB, int lane) {
+  __device__ static void piece(double (&acc)[32], const DPiece &pc, const SView &A,
+                               const SView &B, int lane) {
     const unsigned FULL = 0xffffffffu;
     const int gid = lane >> 2, tig = lane & 3;
     // exponents: lane r for row r of A, lane j for column j of op(B)
     int ea = 0, eb = 0;
     if (lane < pc.M) {
-      const int sh = row_shift(pc.A, lane, pc.lda);
+      const int st = A.start(lane);
       double m = 0.0;
-      for (int k = 0; k < pc.kc; ++k) m = fmax(m, fabs(lds64(sA, lane, sh, k)));
+      for (int k = 0; k < pc.kc; ++k) m = fmax(m, fabs(A.base[st + k]));
       ea = exp_above(m);
     }
     if (lane < pc.N) {
       double m = 0.0;
-      for (int k = 0; k < pc.kc; ++k) m = fmax(m, fabs(opb(pc, sB, k, lane)));
+      for (int k = 0; k < pc.kc; ++k) m = fmax(m, fabs(opb(pc, B, k, lane)));
       eb = exp_above(m);
     }
     int erow[2][2], fb[4], fcol[4][2];
@@ -392,12 +438,12 @@ struct ArithOzaki {
         const int row = 16 * mt + gid + 8 * (rg & 1);
         const int kb = 4 * tig + 16 * (rg >> 1);
         if (mt < MT && row < pc.M) {
-          const int sh = row_shift(pc.A, row, pc.lda);
+          const int st = A.start(row);
 #pragma unroll
           for (int w = 0; w < 4; ++w) {
             const int k = kb + w;
             if (k < pc.kc) {
-              put_digits<S>(ad[mt][rg], lds64(sA, row, sh, k), erow[mt][rg & 1], w);
+              put_digits<S>(ad[mt][rg], A.base[st + k], erow[mt][rg & 1], w);
             }
           }
         }
@@ -417,7 +463,7 @@ struct ArithOzaki {
           for (int w = 0; w < 4; ++w) {
             const int k = 4 * tig + 16 * rg + w;
             if (k < pc.kc) {
-              put_digits<S>(bd[rg], opb(pc, sB, k, col), fb[nt], w);
+              put_digits<S>(bd[rg], opb(pc, B, k, col), fb[nt], w);
             }
           }
         }
@@ -489,15 +535,17 @@ __global__ void __launch_bounds__(DW_WARPS * 32, 1)
     cp_wait<2>();
     __syncwarp();
     const DPiece pc = ring[slot];
-    const unsigned char *sA = wsm + slot * DW_SLOT_BYTES;
-    const unsigned char *sB = sA + DW_HALF;
+    const unsigned char *sbase = wsm + slot * DW_SLOT_BYTES;
+    const SView A{reinterpret_cast<const double *>(sbase), pc.a_flat, pc.a_step, pc.a_sh0,
+                  (pc.flags & PF_LOAD_C) ? pc.ldc : pc.lda};
+    const SView B{reinterpret_cast<const double *>(sbase + pc.b_off), pc.b_flat, pc.b_step,
+                  pc.b_sh0, pc.ldb};
     if (pc.flags & PF_LOAD_C) {
 #pragma unroll
       for (int q = 0; q < 32; ++q) {
         int row, col;
         Arith::pos(q, lane, row, col);
-        acc[q] = (row < pc.M && col < pc.N) ? lds64(sA, row, row_shift(pc.C, row, pc.ldc), col)
-                                            : 0.0;
+        acc[q] = (row < pc.M && col < pc.N) ? A.at(row, col) : 0.0;
       }
       continue;
     }
@@ -510,7 +558,7 @@ __global__ void __launch_bounds__(DW_WARPS * 32, 1)
         for (int q = 0; q < 32; ++q) acc[q] *= pc.beta;
       }
     }
-    Arith::piece(acc, pc, sA, sB, lane);
+    Arith::piece(acc, pc, A, B, lane);
     if (pc.flags & PF_LAST_OF_RUN) {
 #pragma unroll
       for (int q = 0; q < 32; ++q) {
