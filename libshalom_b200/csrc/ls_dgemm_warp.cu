@@ -299,7 +299,6 @@ struct ArithDmma {
   __device__ static void piece(double (&acc)[32], const DPiece &pc, const SView &A,
                                const SView &B, int lane) {
     const int gr = lane >> 2, gc = lane & 3;
-    const int MF = (pc.M + 7) >> 3, NF = (pc.N + 7) >> 3;
     int sa[4], sb[4];  // row starts this thread reads
 #pragma unroll
     for (int mf = 0; mf < 4; ++mf) {
@@ -319,23 +318,23 @@ struct ArithDmma {
 #pragma unroll
       for (int mf = 0; mf < 4; ++mf) {
         const int rr = 8 * mf + gr;
-        a[mf] = (mf < MF && rr < pc.M && k < pc.kc) ? A.base[sa[mf] + k] : 0.0;
+        a[mf] = (rr < pc.M && k < pc.kc) ? A.base[sa[mf] + k] : 0.0;
         if (scale) a[mf] *= pc.alpha;
       }
 #pragma unroll
       for (int nf = 0; nf < 4; ++nf) {
         const int nn = 8 * nf + gr;
         double v = 0.0;
-        if (nf < NF && nn < pc.N && k < pc.kc)
+        if (nn < pc.N && k < pc.kc)
           v = pc.transb ? B.base[sb[nf] + k] : B.base[skb + nn];
         b[nf] = v;
       }
+      // all 16 fragments, branch-free: fragments past M / N multiply zeros
 #pragma unroll
       for (int mf = 0; mf < 4; ++mf)
 #pragma unroll
         for (int nf = 0; nf < 4; ++nf)
-          if (mf < MF && nf < NF)
-            dmma(acc[(mf * 4 + nf) * 2], acc[(mf * 4 + nf) * 2 + 1], a[mf], b[nf]);
+          dmma(acc[(mf * 4 + nf) * 2], acc[(mf * 4 + nf) * 2 + 1], a[mf], b[nf]);
     }
   }
 };
