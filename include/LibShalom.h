@@ -122,6 +122,21 @@ LIBSHALOM_API int LibShalom_get_precision(void);
  * (default), 1 = never split, s > 1 = split K into s slices. */
 LIBSHALOM_API int LibShalom_set_splitk(int splits);
 
+/* Tuning hooks (no counterpart in the reference).  The single and mp entry
+ * points take their tile configuration (plain kernels) and split-K factor
+ * from a table of measured choices per shape class (half-octaves of M, N, K;
+ * written by libshalom_b200/autotune.py on a B200 and compiled in), else from
+ * a cost model.  set_tile_config forces a plain tile configuration
+ * (0..6 FP32: 32x32, 64x64, 128x32, 32x128, 128x64, 64x128, 128x128;
+ * 0..3 FP64: 32x32, 64x64, 128x32, 32x128; -1 = table/model); a value the
+ * data type does not have makes the call fail with
+ * LIBSHALOM_ERR_INVALID_VALUE.  set_autotune(0) ignores the table.
+ * get_plan reports the tile configuration (-1 on the tensor-core path) and
+ * split-K factor of the last single / mp call and the table's entry count. */
+LIBSHALOM_API int LibShalom_set_tile_config(int cfg);
+LIBSHALOM_API int LibShalom_set_autotune(int enable);
+LIBSHALOM_API int LibShalom_get_plan(int *tile_config, int *splits, int *table_entries);
+
 /* Operand staging of the tensor-core kernels: 1 (default) = TMA
  * (cp.async.bulk.tensor) with warp-specialized producer / converter / MMA /
  * epilogue warps whenever the operands are 16-byte aligned with 16-byte row

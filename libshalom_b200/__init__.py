@@ -48,6 +48,7 @@ EXPORTED = (
     "LibShalom_set_stream", "LibShalom_set_sync", "LibShalom_synchronize",
     "LibShalom_set_precision", "LibShalom_get_precision", "LibShalom_set_splitk",
     "LibShalom_set_dgemm_method", "LibShalom_get_dgemm_method",
+    "LibShalom_set_tile_config", "LibShalom_set_autotune", "LibShalom_get_plan",
     "LibShalom_set_tma",
     "LibShalom_finalize",
     "LibShalom_sgemm_batched", "LibShalom_sgemm_batched_strided",
@@ -97,6 +98,9 @@ _SIGS = {
     "LibShalom_get_precision": (_I, []),
     "LibShalom_set_dgemm_method": (_I, [_I, _I]),
     "LibShalom_get_dgemm_method": (_I, []),
+    "LibShalom_set_tile_config": (_I, [_I]),
+    "LibShalom_set_autotune": (_I, [_I]),
+    "LibShalom_get_plan": (_I, [ctypes.POINTER(ctypes.c_int)] * 3),
     "LibShalom_set_splitk": (_I, [_I]),
     "LibShalom_set_tma": (_I, [_I]),
     "LibShalom_finalize": (None, []),
@@ -226,6 +230,22 @@ def set_dgemm_method(method: int, slices: int = 0) -> None:
 
 def get_dgemm_method() -> int:
     return lib().LibShalom_get_dgemm_method()
+
+
+def set_tile_config(cfg: int) -> None:
+    """Force a plain tile configuration (-1: measured table, then cost model)."""
+    _check(lib().LibShalom_set_tile_config(int(cfg)), "LibShalom_set_tile_config")
+
+
+def set_autotune(enable: bool) -> None:
+    _check(lib().LibShalom_set_autotune(1 if enable else 0), "LibShalom_set_autotune")
+
+
+def get_plan():
+    """(tile_config, splits, table_entries) of the last single / mp call."""
+    c, s_, n = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+    lib().LibShalom_get_plan(ctypes.byref(c), ctypes.byref(s_), ctypes.byref(n))
+    return c.value, s_.value, n.value
 
 
 def set_splitk(splits: int) -> None:

@@ -159,10 +159,26 @@ static int gemm_common(int transa, int transb, T *C, const T *A, const T *B, lon
   } else {
     opt.allow_split = false;
   }
-  if (mp && sizeof(T) == 4 && st.precision != LIBSHALOM_PREC_FP32) {
-    rc = tc_sgemm_single((const GemmArgs<float> &)g, st.precision, opt.splits);
+  const bool tc = mp && sizeof(T) == 4 && st.precision != LIBSHALOM_PREC_FP32;
+  // measured shape-class choices, unless forced by the caller
+  const int kind = tc ? (st.precision == LIBSHALOM_PREC_BF16X3 ? TUNE_TC_BF16X3 : TUNE_TC_BF16X6)
+                      : sizeof(T) == 8 ? TUNE_D_SINGLE
+                                       : (mp ? TUNE_S_MP : TUNE_S_SINGLE);
+  int t_cfg = -1, t_splits = 0;
+  const bool hit = st.autotune && !transa && (sizeof(T) == 4 || !mp) &&
+                   tune_lookup(kind, M, N, K, &t_cfg, &t_splits);
+  opt.force_cfg = st.tile_cfg >= 0 ? st.tile_cfg : (hit ? t_cfg : -1);
+  if (hit && mp && st.splitk == 0 && t_splits > 0) opt.splits = t_splits;
+  if (tc) {
+    int used = 0;
+    rc = tc_sgemm_single((const GemmArgs<float> &)g, st.precision, opt.splits, &used);
+    st.last_cfg = -1;
+    st.last_splits = used;
   } else {
-    rc = run_gemm<T>(g, opt, nullptr);
+    SimtPlan plan;
+    rc = run_gemm<T>(g, opt, &plan);
+    st.last_cfg = plan.cfg;
+    st.last_splits = plan.splits;
   }
   if (rc) return rc;
   return finish_launch("gemm");
@@ -278,6 +294,31 @@ int LibShalom_set_dgemm_method(int method, int slices) {
 }
 
 int LibShalom_get_dgemm_method(void) { return state().dgemm_method; }
+
+int LibShalom_set_tile_config(int cfg) {
+  std::lock_guard<std::mutex> lk(state().mu);
+  int rc = LIBSHALOM_SUCCESS;
+  if (cfg < -1 || cfg > 6) rc = LIBSHALOM_ERR_INVALID_VALUE;
+  else state().tile_cfg = cfg;
+  set_error(rc);
+  return rc;
+}
+
+int LibShalom_set_autotune(int enable) {
+  std::lock_guard<std::mutex> lk(state().mu);
+  state().autotune = enable != 0;
+  set_error(LIBSHALOM_SUCCESS);
+  return LIBSHALOM_SUCCESS;
+}
+
+int LibShalom_get_plan(int *tile_config, int *splits, int *table_entries) {
+  std::lock_guard<std::mutex> lk(state().mu);
+  if (tile_config) *tile_config = state().last_cfg;
+  if (splits) *splits = state().last_splits;
+  if (table_entries) *table_entries = tune_table_size();
+  set_error(LIBSHALOM_SUCCESS);
+  return LIBSHALOM_SUCCESS;
+}
 
 int LibShalom_set_splitk(int splits) {
   std::lock_guard<std::mutex> lk(state().mu);

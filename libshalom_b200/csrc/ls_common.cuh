@@ -47,6 +47,9 @@ struct State {
   int dgemm_method = LIBSHALOM_DGEMM_FMA;
   int ozaki_slices = 9;
   int splitk = 0;
+  int tile_cfg = -1;  // forced plain tile configuration (-1: table, then model)
+  int autotune = 1;   // consult the measured shape-class table
+  int last_cfg = -1, last_splits = 0;  // plan of the last single / mp call
   // tensor-core kernels: the TMA warp-specialized variant where the operands
   // allow it (LIBSHALOM_NO_TMA=1 in the environment selects the cp.async one)
   bool use_tma = true;

@@ -293,9 +293,9 @@ int run_gemm(const GemmArgs<T> &g, const SimtOptions &opt, SimtPlan *plan_out) {
   State &st = state();
   int ncfg;
   const CfgInfo *cfgs = Dispatch<T>::cfgs(&ncfg);
-  int cfg = opt.force_cfg >= 0 && opt.force_cfg < ncfg
-                ? opt.force_cfg
-                : pick_cfg(cfgs, ncfg, g.M, g.N, g.K, st.num_sms, st.thread_cap);
+  if (opt.force_cfg >= ncfg) return LIBSHALOM_ERR_INVALID_VALUE;
+  int cfg = opt.force_cfg >= 0 ? opt.force_cfg
+                               : pick_cfg(cfgs, ncfg, g.M, g.N, g.K, st.num_sms, st.thread_cap);
   const long tiles = cdiv(g.M, cfgs[cfg].bm) * cdiv(g.N, cfgs[cfg].bn);
   int splits = opt.allow_split ? pick_splits(tiles, g.K, st.num_sms, st.thread_cap, opt.splits)
                                : 1;

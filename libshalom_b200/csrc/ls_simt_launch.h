@@ -44,4 +44,16 @@ int run_dgemm_warp(const LibShalom_dgemm_entry *entries, long count, int method,
 // floats, device memory owned by the caller).  Allocates nothing.
 int run_gemm_splitk_external(const GemmArgs<float> &g, int splits, float *partial);
 
+// ls_tune.cu: measured choices per shape class (kind, half-octaves of M, N, K)
+enum TuneKind {
+  TUNE_S_SINGLE = 0,   // plain FP32, LibShalom_sgemm (tile configuration)
+  TUNE_S_MP = 1,       // plain FP32, LibShalom_sgemm_mp (tile configuration + split-K)
+  TUNE_D_SINGLE = 2,   // plain FP64, LibShalom_dgemm
+  TUNE_TC_BF16X3 = 3,  // split-BF16 x3, LibShalom_sgemm_mp (split-K)
+  TUNE_TC_BF16X6 = 4,  // split-BF16 x6, LibShalom_sgemm_mp (split-K)
+};
+int half_octave(long x);
+bool tune_lookup(int kind, long M, long N, long K, int *cfg, int *splits);
+int tune_table_size();
+
 }  // namespace ls

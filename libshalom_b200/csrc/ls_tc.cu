@@ -1748,9 +1748,10 @@ static int tc_pick_splits(const GemmArgs<float> &g, int forced) {
   return 1;
 }
 
-int tc_sgemm_single(const GemmArgs<float> &g, int mode, int splits) {
+int tc_sgemm_single(const GemmArgs<float> &g, int mode, int splits, int *used) {
   if (!tc_mode_ok(mode)) return LIBSHALOM_ERR_INVALID_VALUE;
   const int s = g.transa ? 1 : tc_pick_splits(g, splits);
+  if (used) *used = s;
   if (s <= 1) return tc_sgemm_strided(g, 0, 0, 0, 1, mode);
   // K slices as a batch of s partial products into the workspace, then an
   // ordered reduction C = alpha * sum_z partial_z + beta * C

@@ -8,7 +8,9 @@ namespace ls {
 
 // Single (irregular) SGEMM on the tensor cores; `mode` is a
 // LIBSHALOM_PREC_BF16X* value, `splits` as LibShalom_set_splitk.
-int tc_sgemm_single(const GemmArgs<float> &g, int mode, int splits);
+// splits: 0 = chosen here, s > 0 = about s slices; *used (if given) gets the
+// factor launched
+int tc_sgemm_single(const GemmArgs<float> &g, int mode, int splits, int *used = nullptr);
 
 // Uniform batch on the tensor cores.
 int tc_sgemm_strided(const GemmArgs<float> &g, long sA, long sB, long sC, long count, int mode);
