@@ -203,9 +203,56 @@ LIBSHALOM_API int LibShalom_sgemm_mp_noalloc(int transa, int transb, float *C, c
                                              const float *B, long M, long N, long K,
                                              int splits);
 
+/* Plain calls with explicit leading dimensions and scaling (no counterpart in
+ * the reference, whose API has implicit leading dimensions and no alpha /
+ * beta): C = alpha op(A) op(B) + beta C, row-major, lda >= K (A NoTrans) or M
+ * (A Trans), ldb >= N (B NoTrans) or K (B Trans), ldc >= N.  Scheduled like
+ * LibShalom_sgemm_mp (tuning table, split-K; LibShalom_set_precision selects
+ * the split-BF16 path of the FP32 call, which needs transa == NoTrans).
+ * Return the status. */
+LIBSHALOM_API int LibShalom_sgemm_ex(int transa, int transb, long M, long N, long K, float alpha,
+                                     const float *A, long lda, const float *B, long ldb,
+                                     float beta, float *C, long ldc);
+LIBSHALOM_API int LibShalom_dgemm_ex(int transa, int transb, long M, long N, long K,
+                                     double alpha, const double *A, long lda, const double *B,
+                                     long ldb, double beta, double *C, long ldc);
+
 /* Grouped DGEMM (same rules as LibShalom_sgemm_batched).  Arithmetic set by
  * LibShalom_set_dgemm_method. */
 LIBSHALOM_API int LibShalom_dgemm_batched(const LibShalom_dgemm_entry *entries, long count);
+
+/* Stack front end (no counterpart in the reference): a batch described the
+ * way block-sparse chemistry codes keep their multiplication stacks -- data
+ * pools plus per-product element offsets -- instead of per-GEMM pointers.
+ * Product i: C_pool[c_off[i]..] = alpha A_pool[a_off[i]..] op(B_pool[b_off[i]..])
+ * + beta C, dense row-major blocks (lda = K, ldb = N or K for Trans, ldc = N).
+ * M / N / K are device arrays of count sizes, or NULL to give every product
+ * m / n / k.  The offset arrays are device arrays.  Products that name the same
+ * C offset consecutively accumulate in order (a run), exactly as in
+ * LibShalom_dgemm_batched, whose arithmetic (LibShalom_set_dgemm_method) this
+ * call uses.  The struct itself is read on the host. */
+typedef struct LibShalom_dgemm_stack_desc {
+  const double *A_pool;
+  const double *B_pool;
+  double *C_pool;
+  const int32_t *M, *N, *K;
+  int32_t m, n, k;
+  int32_t transb;
+  const int64_t *a_off, *b_off, *c_off;
+  double alpha, beta;
+} LibShalom_dgemm_stack_desc;
+LIBSHALOM_API int LibShalom_dgemm_stack(const LibShalom_dgemm_stack_desc *stack, long count);
+
+/* 2-D convolution front end (no counterpart in the reference; its CNN
+ * benchmark feeds LibShalom_sgemm_mp with im2col shapes): FP32 NCHW
+ * cross-correlation, x [n][c][h][w], weights [oc][c][kh][kw], y [n][oc][oh][ow]
+ * with oh = (h + 2 ph - kh) / sh + 1, ow = (w + 2 pw - kw) / sw + 1, zero
+ * padding; each image is expanded by im2col into a library buffer and
+ * multiplied as the GEMM (oc x c kh kw) (c kh kw x oh ow) on the mp path
+ * (precision mode and tuning apply).  Device pointers; returns the status. */
+LIBSHALOM_API int LibShalom_sconv2d_nchw(const float *x, long n, long c, long h, long w,
+                                         const float *weights, long oc, long kh, long kw,
+                                         long sh, long sw, long ph, long pw, float *y);
 
 /* Arithmetic of LibShalom_dgemm_batched (no counterpart in the reference).
  * Runs whose C block is larger than 32 x 32 always take the FMA kernel. */

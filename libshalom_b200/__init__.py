@@ -49,6 +49,7 @@ EXPORTED = (
     "LibShalom_set_precision", "LibShalom_get_precision", "LibShalom_set_splitk",
     "LibShalom_set_dgemm_method", "LibShalom_get_dgemm_method",
     "LibShalom_set_tile_config", "LibShalom_set_autotune", "LibShalom_get_plan",
+    "LibShalom_sgemm_ex", "LibShalom_dgemm_ex", "LibShalom_dgemm_stack", "LibShalom_sconv2d_nchw",
     "LibShalom_set_tma",
     "LibShalom_finalize",
     "LibShalom_sgemm_batched", "LibShalom_sgemm_batched_strided",
@@ -101,6 +102,12 @@ _SIGS = {
     "LibShalom_set_tile_config": (_I, [_I]),
     "LibShalom_set_autotune": (_I, [_I]),
     "LibShalom_get_plan": (_I, [ctypes.POINTER(ctypes.c_int)] * 3),
+    "LibShalom_sgemm_ex": (_I, [_I, _I, _L, _L, _L, ctypes.c_float, _P, _L, _P, _L,
+                                ctypes.c_float, _P, _L]),
+    "LibShalom_dgemm_ex": (_I, [_I, _I, _L, _L, _L, ctypes.c_double, _P, _L, _P, _L,
+                                ctypes.c_double, _P, _L]),
+    "LibShalom_dgemm_stack": (_I, [_P, _L]),
+    "LibShalom_sconv2d_nchw": (_I, [_P, _L, _L, _L, _L, _P, _L, _L, _L, _L, _L, _L, _L, _P]),
     "LibShalom_set_splitk": (_I, [_I]),
     "LibShalom_set_tma": (_I, [_I]),
     "LibShalom_finalize": (None, []),
@@ -239,6 +246,56 @@ def set_tile_config(cfg: int) -> None:
 
 def set_autotune(enable: bool) -> None:
     _check(lib().LibShalom_set_autotune(1 if enable else 0), "LibShalom_set_autotune")
+
+
+def sgemm_ex(transa, transb, M, N, K, alpha, A, lda, B, ldb, beta, C, ldc, check=True) -> int:
+    """C = alpha op(A) op(B) + beta C with explicit leading dimensions (FP32)."""
+    st = lib().LibShalom_sgemm_ex(transa, transb, M, N, K, alpha, _ptr(A), lda, _ptr(B), ldb,
+                                  beta, _ptr(C), ldc)
+    if check:
+        _check(st, "LibShalom_sgemm_ex")
+    return st
+
+
+def dgemm_ex(transa, transb, M, N, K, alpha, A, lda, B, ldb, beta, C, ldc, check=True) -> int:
+    """C = alpha op(A) op(B) + beta C with explicit leading dimensions (FP64)."""
+    st = lib().LibShalom_dgemm_ex(transa, transb, M, N, K, alpha, _ptr(A), lda, _ptr(B), ldb,
+                                  beta, _ptr(C), ldc)
+    if check:
+        _check(st, "LibShalom_dgemm_ex")
+    return st
+
+
+class DgemmStack(ctypes.Structure):
+    """LibShalom_dgemm_stack (host struct of device pointers)."""
+    _fields_ = [("A_pool", ctypes.c_void_p), ("B_pool", ctypes.c_void_p),
+                ("C_pool", ctypes.c_void_p), ("M", ctypes.c_void_p), ("N", ctypes.c_void_p),
+                ("K", ctypes.c_void_p), ("m", ctypes.c_int32), ("n", ctypes.c_int32),
+                ("k", ctypes.c_int32), ("transb", ctypes.c_int32), ("a_off", ctypes.c_void_p),
+                ("b_off", ctypes.c_void_p), ("c_off", ctypes.c_void_p),
+                ("alpha", ctypes.c_double), ("beta", ctypes.c_double)]
+
+
+def dgemm_stack(A_pool, B_pool, C_pool, a_off, b_off, c_off, count, m=0, n=0, k=0, M=None,
+                N=None, K=None, transb=0, alpha=1.0, beta=1.0, check=True) -> int:
+    """Batched DGEMM from pools and per-product offsets (device arrays)."""
+    st_ = DgemmStack(_ptr(A_pool), _ptr(B_pool), _ptr(C_pool),
+                     _ptr(M) if M is not None else None, _ptr(N) if N is not None else None,
+                     _ptr(K) if K is not None else None, m, n, k, transb,
+                     _ptr(a_off), _ptr(b_off), _ptr(c_off), alpha, beta)
+    st = lib().LibShalom_dgemm_stack(ctypes.byref(st_), count)
+    if check:
+        _check(st, "LibShalom_dgemm_stack")
+    return st
+
+
+def sconv2d_nchw(x, n, c, h, w, weights, oc, kh, kw, sh, sw, ph, pw, y, check=True) -> int:
+    """FP32 NCHW convolution through im2col and the mp GEMM path."""
+    st = lib().LibShalom_sconv2d_nchw(_ptr(x), n, c, h, w, _ptr(weights), oc, kh, kw, sh, sw,
+                                      ph, pw, _ptr(y))
+    if check:
+        _check(st, "LibShalom_sconv2d_nchw")
+    return st
 
 
 def get_plan():

@@ -9,6 +9,7 @@
 #include <unordered_map>
 
 #include "ls_common.cuh"
+#include "ls_frontend.h"
 #include "ls_simt_launch.h"
 #include "ls_tc_launch.h"
 
@@ -127,14 +128,46 @@ int finish_launch(const char *what) {
   return LIBSHALOM_SUCCESS;
 }
 
+// Buffer of the front ends (grown on demand like the workspace).
+static int frontend_buffer(size_t bytes, void **out) {
+  State &st = state();
+  if (bytes < 256) bytes = 256;
+  if (st.fe && st.fe_bytes >= bytes && st.fe_device == st.device) {
+    *out = st.fe;
+    return LIBSHALOM_SUCCESS;
+  }
+  if (st.fe) {
+    LS_CUDA_TRY(cudaStreamSynchronize(st.stream));
+    cudaFree(st.fe);
+    st.fe = nullptr;
+    st.fe_bytes = 0;
+  }
+  const size_t want = std::max(bytes, (size_t)1 << 20);
+  if (cudaMalloc(&st.fe, want) != cudaSuccess) {
+    cudaGetLastError();
+    st.fe = nullptr;
+    return LIBSHALOM_ERR_ALLOC;
+  }
+  st.fe_bytes = want;
+  st.fe_device = st.device;
+  *out = st.fe;
+  return LIBSHALOM_SUCCESS;
+}
+
+// lda / ldb / ldc = 0: the row-major defaults of the drop-in calls
 template <typename T>
 static int gemm_common(int transa, int transb, T *C, const T *A, const T *B, long M, long N,
-                       long K, bool mp) {
+                       long K, bool mp, T alpha = T(1), T beta = T(0), long lda = 0,
+                       long ldb = 0, long ldc = 0) {
   if ((transa != NoTrans && transa != Trans) || (transb != NoTrans && transb != Trans))
     return LIBSHALOM_ERR_INVALID_VALUE;
   if (M < 0 || N < 0 || K < 0) return LIBSHALOM_ERR_INVALID_VALUE;
+  if (lda < 0 || ldb < 0 || ldc < 0) return LIBSHALOM_ERR_INVALID_VALUE;
+  if ((lda && lda < (transa ? M : K)) || (ldb && ldb < (transb ? K : N)) || (ldc && ldc < N))
+    return LIBSHALOM_ERR_INVALID_VALUE;
   if (M == 0 || N == 0) return LIBSHALOM_SUCCESS;
   if (!C || (K > 0 && (!A || !B))) return LIBSHALOM_ERR_INVALID_VALUE;
+  if (lda > INT32_MAX || ldb > INT32_MAX || ldc > INT32_MAX) return LIBSHALOM_ERR_INVALID_VALUE;
   // int32 tile indices inside the kernels
   if (M > (1L << 30) || N > (1L << 30) || K > (1L << 40)) return LIBSHALOM_ERR_INVALID_VALUE;
   int rc = ensure_device();
@@ -144,10 +177,10 @@ static int gemm_common(int transa, int transb, T *C, const T *A, const T *B, lon
   g.A = A; g.B = B; g.C = C;
   g.M = M; g.N = N; g.K = K;
   g.transa = transa; g.transb = transb;
-  g.lda = transa ? M : K;
-  g.ldb = transb ? K : N;
-  g.ldc = N;
-  g.alpha = T(1); g.beta = T(0);
+  g.lda = lda ? lda : (transa ? M : K);
+  g.ldb = ldb ? ldb : (transb ? K : N);
+  g.ldc = ldc ? ldc : N;
+  g.alpha = alpha; g.beta = beta;
   SimtOptions opt;
   if (mp) {
     opt.kblock = true;
@@ -339,13 +372,15 @@ int LibShalom_set_tma(int enable) {
 void LibShalom_finalize(void) {
   std::lock_guard<std::mutex> lk(state().mu);
   State &st = state();
-  if (st.ws) {
-    cudaStreamSynchronize(st.stream);
-    cudaFree(st.ws);
-  }
+  if (st.ws || st.fe) cudaStreamSynchronize(st.stream);
+  if (st.ws) cudaFree(st.ws);
+  if (st.fe) cudaFree(st.fe);
   st.ws = nullptr;
   st.ws_bytes = 0;
   st.ws_device = -1;
+  st.fe = nullptr;
+  st.fe_bytes = 0;
+  st.fe_device = -1;
   set_error(LIBSHALOM_SUCCESS);
 }
 
@@ -403,6 +438,85 @@ int LibShalom_dgemm_batched(const LibShalom_dgemm_entry *entries, long count) {
              ? run_grouped_d(entries, count)
              : run_dgemm_warp(entries, count, st.dgemm_method, st.ozaki_slices);
     if (!rc) rc = finish_launch("dgemm_batched");
+  }
+  set_error(rc);
+  return rc;
+}
+
+int LibShalom_sgemm_ex(int transa, int transb, long M, long N, long K, float alpha,
+                       const float *A, long lda, const float *B, long ldb, float beta, float *C,
+                       long ldc) {
+  std::lock_guard<std::mutex> lk(state().mu);
+  const int rc = gemm_common<float>(transa, transb, C, A, B, M, N, K, true, alpha, beta,
+                                    std::max(lda, 1L), std::max(ldb, 1L), std::max(ldc, 1L));
+  set_error(rc);
+  return rc;
+}
+
+int LibShalom_dgemm_ex(int transa, int transb, long M, long N, long K, double alpha,
+                       const double *A, long lda, const double *B, long ldb, double beta,
+                       double *C, long ldc) {
+  std::lock_guard<std::mutex> lk(state().mu);
+  const int rc = gemm_common<double>(transa, transb, C, A, B, M, N, K, true, alpha, beta,
+                                     std::max(lda, 1L), std::max(ldb, 1L), std::max(ldc, 1L));
+  set_error(rc);
+  return rc;
+}
+
+int LibShalom_dgemm_stack(const LibShalom_dgemm_stack_desc *stack, long count) {
+  std::lock_guard<std::mutex> lk(state().mu);
+  int rc = LIBSHALOM_SUCCESS;
+  if (!stack || count < 0 || count > (1L << 30)) rc = LIBSHALOM_ERR_INVALID_VALUE;
+  else if (count > 0 && (!stack->a_off || !stack->b_off || !stack->c_off || !stack->C_pool ||
+                         ((!stack->M && stack->m < 0) || (!stack->N && stack->n < 0) ||
+                          (!stack->K && stack->k < 0)) ||
+                         (stack->transb != NoTrans && stack->transb != Trans)))
+    rc = LIBSHALOM_ERR_INVALID_VALUE;
+  else if (count > 0 && !(rc = ensure_device())) {
+    void *buf = nullptr;
+    rc = frontend_buffer(sizeof(LibShalom_dgemm_entry) * (size_t)count, &buf);
+    if (!rc) {
+      StackArgs a;
+      a.A = stack->A_pool; a.B = stack->B_pool; a.C = stack->C_pool;
+      a.M = stack->M; a.N = stack->N; a.K = stack->K;
+      a.m = stack->m; a.n = stack->n; a.k = stack->k; a.transb = stack->transb;
+      a.a_off = stack->a_off; a.b_off = stack->b_off; a.c_off = stack->c_off;
+      a.alpha = stack->alpha; a.beta = stack->beta;
+      auto *ent = static_cast<LibShalom_dgemm_entry *>(buf);
+      rc = stack_to_entries(a, count, ent);
+      if (!rc) {
+        const State &st = state();
+        rc = st.dgemm_method == LIBSHALOM_DGEMM_FMA
+                 ? run_grouped_d(ent, count)
+                 : run_dgemm_warp(ent, count, st.dgemm_method, st.ozaki_slices);
+      }
+      if (!rc) rc = finish_launch("dgemm_stack");
+    }
+  }
+  set_error(rc);
+  return rc;
+}
+
+int LibShalom_sconv2d_nchw(const float *x, long n, long c, long h, long w, const float *wt,
+                           long oc, long kh, long kw, long sh, long sw, long ph, long pw,
+                           float *y) {
+  std::lock_guard<std::mutex> lk(state().mu);
+  int rc = LIBSHALOM_SUCCESS;
+  if (n < 0 || c <= 0 || h <= 0 || w <= 0 || oc <= 0 || kh <= 0 || kw <= 0 || sh <= 0 ||
+      sw <= 0 || ph < 0 || pw < 0 || !x || !wt || !y)
+    rc = LIBSHALOM_ERR_INVALID_VALUE;
+  const long oh = (h + 2 * ph - kh) / sh + 1, ow = (w + 2 * pw - kw) / sw + 1;
+  if (!rc && (h + 2 * ph < kh || w + 2 * pw < kw)) rc = LIBSHALOM_ERR_INVALID_VALUE;
+  if (!rc && n > 0 && !(rc = ensure_device())) {
+    const long K = c * kh * kw, P = oh * ow;
+    void *buf = nullptr;
+    rc = frontend_buffer(sizeof(float) * (size_t)K * P, &buf);
+    float *col = static_cast<float *>(buf);
+    for (long i = 0; !rc && i < n; ++i) {
+      rc = im2col(x + i * c * h * w, c, h, w, kh, kw, sh, sw, ph, pw, oh, ow, col);
+      // y_i [oc][P] = wt [oc][K] col [K][P]
+      if (!rc) rc = gemm_common<float>(NoTrans, NoTrans, y + i * oc * P, wt, col, oc, P, K, true);
+    }
   }
   set_error(rc);
   return rc;

@@ -57,6 +57,11 @@ struct State {
   void *ws = nullptr;
   size_t ws_bytes = 0;
   int ws_device = -1;
+  // front-end buffer (stack entries, im2col columns): separate from the
+  // workspace, which the GEMM paths the front ends call use themselves
+  void *fe = nullptr;
+  size_t fe_bytes = 0;
+  int fe_device = -1;
 };
 
 State &state();
