@@ -511,12 +511,25 @@ def wl_single(args):
     for _ in range(args.steps):
         ls.sgemm(0, 1, C, A, B, 80, 80, 80)
     ms_sync = (time.perf_counter() - t0) / args.steps * 1e3
+    # the same calls replayed from the library's graph cache
+    ls.set_graph_cache(True)
+    for _ in range(max(args.warmup, 3)):
+        ls.sgemm(0, 1, C, A, B, 80, 80, 80)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        ls.sgemm(0, 1, C, A, B, 80, 80, 80)
+    ms_sync_graph = (time.perf_counter() - t0) / args.steps * 1e3
     ls.set_sync(False)
+    ms_async_graph = _time_events(torch, s, lambda: ls.sgemm(0, 1, C, A, B, 80, 80, 80),
+                                  args.steps, args.warmup)
+    ls.set_graph_cache(False)
     _emit("single SGEMM NT 80^3 GFLOP/s (synchronous calls, as the reference API)",
           flops / (ms_sync / 1e3) / 1e9, "GFLOP/s", ms_sync, args,
           {"workload": "LibShalom_sgemm(NoTrans, Trans) M=N=K=80, C overwritten, one call per step"},
           4.0 * 3 * 80 * 80,
           {"dtype": "f32", "latency_us_sync": ms_sync * 1e3, "latency_us_stream": ms_async * 1e3,
+           "latency_us_sync_graph_cache": ms_sync_graph * 1e3,
+           "latency_us_stream_graph_cache": ms_async_graph * 1e3,
            "gflops_stream_ordered": flops / (ms_async / 1e3) / 1e9, "gpu_launches": args.steps})
 
 

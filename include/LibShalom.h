@@ -134,6 +134,16 @@ LIBSHALOM_API int LibShalom_set_splitk(int splits);
  * get_plan reports the tile configuration (-1 on the tensor-core path) and
  * split-K factor of the last single / mp call and the table's entry count. */
 LIBSHALOM_API int LibShalom_set_tile_config(int cfg);
+
+/* Graph cache (no counterpart in the reference): with enable != 0 and a
+ * non-default stream set, a LibShalom_sgemm / _sgemm_mp / _dgemm call whose
+ * pointers, sizes and library settings repeat is captured into a CUDA graph
+ * the second time and replayed by one graph launch from then on (up to 256
+ * cached calls; a call that makes the library's workspace grow recaptures).
+ * The data behind the pointers may change between calls.  Replays do not
+ * report an expired device-side wait as LIBSHALOM_ERR_DEVICE_TIMEOUT.
+ * enable == 0 (default) frees the cached graphs. */
+LIBSHALOM_API int LibShalom_set_graph_cache(int enable);
 LIBSHALOM_API int LibShalom_set_autotune(int enable);
 LIBSHALOM_API int LibShalom_get_plan(int *tile_config, int *splits, int *table_entries);
 

@@ -50,6 +50,7 @@ EXPORTED = (
     "LibShalom_set_dgemm_method", "LibShalom_get_dgemm_method",
     "LibShalom_set_tile_config", "LibShalom_set_autotune", "LibShalom_get_plan",
     "LibShalom_sgemm_ex", "LibShalom_dgemm_ex", "LibShalom_dgemm_stack", "LibShalom_sconv2d_nchw",
+    "LibShalom_set_graph_cache",
     "LibShalom_set_tma",
     "LibShalom_finalize",
     "LibShalom_sgemm_batched", "LibShalom_sgemm_batched_strided",
@@ -107,6 +108,7 @@ _SIGS = {
     "LibShalom_dgemm_ex": (_I, [_I, _I, _L, _L, _L, ctypes.c_double, _P, _L, _P, _L,
                                 ctypes.c_double, _P, _L]),
     "LibShalom_dgemm_stack": (_I, [_P, _L]),
+    "LibShalom_set_graph_cache": (_I, [_I]),
     "LibShalom_sconv2d_nchw": (_I, [_P, _L, _L, _L, _L, _P, _L, _L, _L, _L, _L, _L, _L, _P]),
     "LibShalom_set_splitk": (_I, [_I]),
     "LibShalom_set_tma": (_I, [_I]),
@@ -296,6 +298,11 @@ def sconv2d_nchw(x, n, c, h, w, weights, oc, kh, kw, sh, sw, ph, pw, y, check=Tr
     if check:
         _check(st, "LibShalom_sconv2d_nchw")
     return st
+
+
+def set_graph_cache(enable: bool) -> None:
+    """Replay repeated identical single / mp calls from cached CUDA graphs."""
+    _check(lib().LibShalom_set_graph_cache(1 if enable else 0), "LibShalom_set_graph_cache")
 
 
 def get_plan():

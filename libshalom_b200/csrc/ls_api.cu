@@ -77,6 +77,7 @@ int workspace(size_t bytes, void **out) {
   }
   st.ws_bytes = want;
   st.ws_device = st.device;
+  ++st.ws_generation;  // graphs captured with the old buffer are stale
   *out = st.ws;
   return LIBSHALOM_SUCCESS;
 }
@@ -217,6 +218,103 @@ static int gemm_common(int transa, int transb, T *C, const T *A, const T *B, lon
   return finish_launch("gemm");
 }
 
+// ---------------------------------------------------------------------------
+// Graph cache of the drop-in single / mp calls.  A call whose arguments and
+// library settings repeat exactly is captured into a CUDA graph the second
+// time it is seen (the first run has already sized the workspace) and
+// replayed from then on with one cudaGraphLaunch.  Entries remember the
+// workspace generation they were captured with; a workspace that moved
+// invalidates them.  Needs a non-default stream (LibShalom_set_stream).
+// ---------------------------------------------------------------------------
+struct GraphKey {
+  int kind, transa, transb, precision, tile_cfg, autotune, splitk, ways_m, ways_n, device;
+  const void *A, *B, *C;
+  long M, N, K;
+  cudaStream_t stream;
+  bool operator==(const GraphKey &o) const { return memcmp(this, &o, sizeof(*this)) == 0; }
+};
+struct GraphKeyHash {
+  size_t operator()(const GraphKey &k) const {
+    const unsigned char *p = reinterpret_cast<const unsigned char *>(&k);
+    size_t h = 1469598103934665603ull;
+    for (size_t i = 0; i < sizeof(k); ++i) h = (h ^ p[i]) * 1099511628211ull;
+    return h;
+  }
+};
+struct GraphEntry {
+  int uses = 0;
+  unsigned generation = 0;
+  cudaGraphExec_t exec = nullptr;
+};
+static std::unordered_map<GraphKey, GraphEntry, GraphKeyHash> &graph_cache() {
+  static std::unordered_map<GraphKey, GraphEntry, GraphKeyHash> m;
+  return m;
+}
+static void graph_cache_clear() {
+  for (auto &kv : graph_cache())
+    if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
+  graph_cache().clear();
+}
+constexpr size_t kGraphCacheMax = 256;
+
+template <typename T>
+static int gemm_cached(int kind, int transa, int transb, T *C, const T *A, const T *B, long M,
+                       long N, long K, bool mp) {
+  State &st = state();
+  if (!st.graph_cache || st.stream == nullptr || M <= 0 || N <= 0)
+    return gemm_common<T>(transa, transb, C, A, B, M, N, K, mp);
+  int rc = ensure_device();
+  if (rc) return rc;
+  GraphKey key;
+  memset(&key, 0, sizeof(key));  // padding bytes take part in the hash
+  key.kind = kind; key.transa = transa; key.transb = transb; key.precision = st.precision;
+  key.tile_cfg = st.tile_cfg; key.autotune = st.autotune; key.splitk = st.splitk;
+  key.ways_m = st.ways_m; key.ways_n = st.ways_n; key.device = st.device;
+  key.A = A; key.B = B; key.C = C; key.M = M; key.N = N; key.K = K; key.stream = st.stream;
+  auto &cache = graph_cache();
+  auto it = cache.find(key);
+  if (it != cache.end() && it->second.exec && it->second.generation == st.ws_generation) {
+    st.ways_m = st.ways_n = 0;  // one-shot, as on the direct path
+    LS_CUDA_TRY(cudaGraphLaunch(it->second.exec, st.stream));
+    return finish_launch("gemm (graph)");
+  }
+  if (it == cache.end()) {
+    if (cache.size() >= kGraphCacheMax) graph_cache_clear();
+    cache[key].uses = 1;
+    return gemm_common<T>(transa, transb, C, A, B, M, N, K, mp);  // first sight: run it
+  }
+  // second sight (or stale graph): capture this run, then launch the graph
+  GraphEntry &ge = it->second;
+  if (ge.exec) {
+    cudaGraphExecDestroy(ge.exec);
+    ge.exec = nullptr;
+  }
+  const int sync = st.sync;
+  st.sync = 0;  // no host synchronisation inside the capture
+  LS_CUDA_TRY(cudaStreamBeginCapture(st.stream, cudaStreamCaptureModeThreadLocal));
+  rc = gemm_common<T>(transa, transb, C, A, B, M, N, K, mp);
+  cudaGraph_t graph = nullptr;
+  const cudaError_t ce = cudaStreamEndCapture(st.stream, &graph);
+  st.sync = sync;
+  if (rc || ce != cudaSuccess || !graph) {
+    if (graph) cudaGraphDestroy(graph);
+    cudaGetLastError();
+    cache.erase(key);
+    return rc ? rc : LIBSHALOM_ERR_CUDA;
+  }
+  const cudaError_t ie = cudaGraphInstantiate(&ge.exec, graph, 0);
+  cudaGraphDestroy(graph);
+  if (ie != cudaSuccess) {
+    cudaGetLastError();
+    cache.erase(key);
+    return LIBSHALOM_ERR_CUDA;
+  }
+  ge.generation = st.ws_generation;
+  ++ge.uses;
+  LS_CUDA_TRY(cudaGraphLaunch(ge.exec, st.stream));
+  return finish_launch("gemm (graph)");
+}
+
 }  // namespace ls
 
 using namespace ls;
@@ -226,19 +324,19 @@ extern "C" {
 void LibShalom_sgemm(int transa, int transb, float *C, float *A, float *B, long M, long N,
                      long K) {
   std::lock_guard<std::mutex> lk(state().mu);
-  set_error(gemm_common<float>(transa, transb, C, A, B, M, N, K, false));
+  set_error(gemm_cached<float>(0, transa, transb, C, A, B, M, N, K, false));
 }
 
 void LibShalom_sgemm_mp(int transa, int transb, float *C, float *A, float *B, long M, long N,
                         long K) {
   std::lock_guard<std::mutex> lk(state().mu);
-  set_error(gemm_common<float>(transa, transb, C, A, B, M, N, K, true));
+  set_error(gemm_cached<float>(1, transa, transb, C, A, B, M, N, K, true));
 }
 
 void LibShalom_dgemm(int transa, int transb, double *C, double *A, double *B, long M, long N,
                      long K) {
   std::lock_guard<std::mutex> lk(state().mu);
-  set_error(gemm_common<double>(transa, transb, C, A, B, M, N, K, false));
+  set_error(gemm_cached<double>(2, transa, transb, C, A, B, M, N, K, false));
 }
 
 void LibShalom_set_thread_nums(int num) {
@@ -328,6 +426,14 @@ int LibShalom_set_dgemm_method(int method, int slices) {
 
 int LibShalom_get_dgemm_method(void) { return state().dgemm_method; }
 
+int LibShalom_set_graph_cache(int enable) {
+  std::lock_guard<std::mutex> lk(state().mu);
+  state().graph_cache = enable != 0;
+  if (!enable) graph_cache_clear();
+  set_error(LIBSHALOM_SUCCESS);
+  return LIBSHALOM_SUCCESS;
+}
+
 int LibShalom_set_tile_config(int cfg) {
   std::lock_guard<std::mutex> lk(state().mu);
   int rc = LIBSHALOM_SUCCESS;
@@ -373,6 +479,7 @@ void LibShalom_finalize(void) {
   std::lock_guard<std::mutex> lk(state().mu);
   State &st = state();
   if (st.ws || st.fe) cudaStreamSynchronize(st.stream);
+  graph_cache_clear();
   if (st.ws) cudaFree(st.ws);
   if (st.fe) cudaFree(st.fe);
   st.ws = nullptr;

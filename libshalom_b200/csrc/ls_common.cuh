@@ -62,6 +62,8 @@ struct State {
   void *fe = nullptr;
   size_t fe_bytes = 0;
   int fe_device = -1;
+  unsigned ws_generation = 0;  // bumped whenever the workspace moves
+  int graph_cache = 0;         // replay repeated identical single / mp calls
 };
 
 State &state();
