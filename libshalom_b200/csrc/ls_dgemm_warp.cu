@@ -61,7 +61,11 @@ struct __align__(16) DPiece {
   // in doubles between row starts, and the source address's double parity
   int b_off, a_flat, a_step, a_sh0, b_flat, b_step, b_sh0, pad_;
 };
-constexpr int DW_WARP_BYTES = DW_SLOTS * DW_SLOT_BYTES + DW_SLOTS * (int)sizeof(DPiece);
+// per warp: slots, piece ring, one mbarrier per slot
+constexpr int DW_RING_OFF = DW_SLOTS * DW_SLOT_BYTES;
+constexpr int DW_BAR_OFF = DW_RING_OFF + DW_SLOTS * (int)sizeof(DPiece);
+constexpr int DW_WARP_BYTES = (DW_BAR_OFF + DW_SLOTS * 8 + 127) & ~127;  // slots stay 16-byte aligned
+static_assert(DW_SLOT_BYTES % 16 == 0 && DW_WARP_BYTES % 16 == 0, "bulk-copy destinations");
 constexpr int DW_SMEM = DW_WARPS * DW_WARP_BYTES;
 static_assert(DW_SMEM <= 232448, "per-CTA shared memory");
 
@@ -93,7 +97,6 @@ __global__ void k_dw_plan(const LibShalom_dgemm_entry *e, long count, DwPlan pl)
 __device__ __forceinline__ void cp16(uint32_t saddr, uintptr_t g) {
   asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(saddr), "l"(g) : "memory");
 }
-__device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
 template <int N>
 __device__ __forceinline__ void cp_wait() {
   asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
@@ -113,10 +116,27 @@ __device__ __forceinline__ int stage_bytes(int rows, int len, int ld) {
   return can_flat(rows, len, ld) ? flat_bytes(rows, len, ld) : rows * win_pitch(len);
 }
 
-// copy the staged matrix into dst with 16-byte cp.async (only 16-byte blocks
-// that hold at least one element are read); returns the layout fields
+__device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
+  asm volatile("mbarrier.expect_tx.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void bulk_copy(uint32_t dst, uintptr_t src, uint32_t bytes,
+                                          uint32_t bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+          dst),
+      "l"(src), "r"(bytes), "r"(bar)
+      : "memory");
+}
+__device__ __forceinline__ void cp_async_arrive(uint32_t bar) {
+  asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];" ::"r"(bar) : "memory");
+}
+
+// copy the staged matrix into dst (only 16-byte blocks that hold at least one
+// element are read): a contiguous one as a single bulk copy issued by lane 0
+// (its bytes are added to the slot barrier's transaction count), row windows
+// with 16-byte cp.async by all lanes; returns the layout fields
 __device__ __forceinline__ void stage_mat(uint32_t dst, const double *p, int rows, int len, int ld,
-                                      int lane, int &flat, int &step, int &sh0) {
+                                      int lane, int &flat, int &step, int &sh0, uint32_t bar) {
   const uintptr_t a0 = reinterpret_cast<uintptr_t>(p);
   sh0 = (int)((a0 >> 3) & 1);
   if (rows <= 0 || len <= 0) {
@@ -127,8 +147,11 @@ __device__ __forceinline__ void stage_mat(uint32_t dst, const double *p, int row
     flat = 1; step = ld;
     const uintptr_t w0 = a0 & ~uintptr_t(15);
     const uintptr_t end = a0 + 8 * ((uintptr_t)(rows - 1) * ld + len);
-    const int chunks = (int)((end - w0 + 15) >> 4);
-    for (int q = lane; q < chunks; q += 32) cp16(dst + 16 * q, w0 + 16 * q);
+    const uint32_t bytes = (uint32_t)(((end - w0 + 15) >> 4) << 4);
+    if (lane == 0) {
+      mbar_expect_tx(bar, bytes);
+      bulk_copy(dst, w0, bytes, bar);
+    }
     return;
   }
   flat = 0;
@@ -215,8 +238,9 @@ struct DLoader {
   __device__ bool issue(unsigned char *wsm, int slot, int lane) {
     if (done) return false;
     unsigned char *sbuf = wsm + slot * DW_SLOT_BYTES;
-    DPiece *ring = reinterpret_cast<DPiece *>(wsm + DW_SLOTS * DW_SLOT_BYTES);
+    DPiece *ring = reinterpret_cast<DPiece *>(wsm + DW_RING_OFF);
     const uint32_t sa = (uint32_t)__cvta_generic_to_shared(sbuf);
+    const uint32_t bar = (uint32_t)__cvta_generic_to_shared(wsm + DW_BAR_OFF + 8 * slot);
     DPiece pc;
     pc.M = M; pc.N = N; pc.C = C; pc.ldc = ldc;
     if (stage == 0) {
@@ -225,7 +249,7 @@ struct DLoader {
       pc.A = nullptr; pc.B = nullptr; pc.kc = 0; pc.lda = pc.ldb = 0; pc.transb = 0;
       pc.alpha = 1.0; pc.beta = 1.0;
       pc.b_off = 0; pc.b_flat = 1; pc.b_step = 0; pc.b_sh0 = 0;
-      stage_mat(sa, C, M, N, ldc, lane, pc.a_flat, pc.a_step, pc.a_sh0);
+      stage_mat(sa, C, M, N, ldc, lane, pc.a_flat, pc.a_step, pc.a_sh0, bar);
       stage = 1;
     } else {
       const int src = p - base;
@@ -255,11 +279,11 @@ struct DLoader {
       pc.lda = e.lda; pc.ldb = e.ldb; pc.transb = e.transb;
       pc.alpha = e.alpha; pc.beta = e.beta;
       pc.b_off = (stage_bytes(M, kc, e.lda) + 15) & ~15;
-      stage_mat(sa, pc.A, M, kc, pc.lda, lane, pc.a_flat, pc.a_step, pc.a_sh0);
+      stage_mat(sa, pc.A, M, kc, pc.lda, lane, pc.a_flat, pc.a_step, pc.a_sh0, bar);
       if (e.transb)
-        stage_mat(sa + pc.b_off, pc.B, N, kc, pc.ldb, lane, pc.b_flat, pc.b_step, pc.b_sh0);
+        stage_mat(sa + pc.b_off, pc.B, N, kc, pc.ldb, lane, pc.b_flat, pc.b_step, pc.b_sh0, bar);
       else
-        stage_mat(sa + pc.b_off, pc.B, kc, N, pc.ldb, lane, pc.b_flat, pc.b_step, pc.b_sh0);
+        stage_mat(sa + pc.b_off, pc.B, kc, N, pc.ldb, lane, pc.b_flat, pc.b_step, pc.b_sh0, bar);
       // advance (a product with K = 0 is one empty piece)
       kc0 += max(kc, 1);
       if (kc0 >= e.K) {
@@ -275,6 +299,9 @@ struct DLoader {
       }
     }
     if (lane == 0) ring[slot] = pc;
+    // the slot's phase completes when every lane's cp.async copies and the
+    // bulk copies' bytes have landed
+    cp_async_arrive(bar);
     return true;
   }
 };
@@ -500,6 +527,26 @@ struct ArithOzaki {
   }
 };
 
+// device status word: a slot barrier that never completed
+__device__ unsigned g_dw_err;
+
+// bounded wait for a phase of a slot barrier (about a second with back-off)
+__device__ __forceinline__ bool bar_wait(uint64_t *bar, uint32_t parity) {
+  const uint32_t a = (uint32_t)__cvta_generic_to_shared(bar);
+  for (uint32_t it = 0; it < (1u << 22); ++it) {
+    uint32_t done;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.b32 %0, 1, 0, p;\n\t}"
+        : "=r"(done)
+        : "r"(a), "r"(parity)
+        : "memory");
+    if (done) return true;
+    if (it > 64) __nanosleep(it < 4096 ? 32 : 256);
+  }
+  return false;
+}
+
 // ---------------------------------------------------------------------------
 // The warp kernel: load side two pieces ahead, compute side per piece.
 // ---------------------------------------------------------------------------
@@ -510,19 +557,27 @@ __global__ void __launch_bounds__(DW_WARPS * 32, 1)
   extern __shared__ __align__(16) unsigned char dsm[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   unsigned char *wsm = dsm + warp * DW_WARP_BYTES;
-  const DPiece *ring = reinterpret_cast<const DPiece *>(wsm + DW_SLOTS * DW_SLOT_BYTES);
+  const DPiece *ring = reinterpret_cast<const DPiece *>(wsm + DW_RING_OFF);
+  uint64_t *bars = reinterpret_cast<uint64_t *>(wsm + DW_BAR_OFF);
+  if (lane == 0) {
+    for (int i = 0; i < DW_SLOTS; ++i)
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 32;" ::"r"(
+                       (uint32_t)__cvta_generic_to_shared(&bars[i]))
+                   : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncwarp();
   const long n_runs = (long)*n_runs_p;
   DLoader ld;
   ld.init(entries, run_first, run_len, n_runs, (long)blockIdx.x * DW_WARPS + warp,
           (long)gridDim.x * DW_WARPS, lane);
 
-  // prologue: two pieces in flight (one commit group per piece slot, also
-  // when empty, so the group count stays in step with the piece count)
+  // prologue: two pieces in flight; piece i completes phase i / DW_SLOTS of
+  // the barrier of slot i % DW_SLOTS
   long n_issued = 0;
-  for (int s = 0; s < 2; ++s) {
+  for (int s = 0; s < 2; ++s)
     if (ld.issue(wsm, s, lane)) ++n_issued;
-    cp_commit();
-  }
+  bool ok = true;
   double acc[32];
 #pragma unroll
   for (int i = 0; i < 32; ++i) acc[i] = 0.0;
@@ -530,8 +585,11 @@ __global__ void __launch_bounds__(DW_WARPS * 32, 1)
     const int slot = (int)(i % DW_SLOTS);
     __syncwarp();  // every lane is done with the slot refilled next
     if (ld.issue(wsm, (int)((i + 2) % DW_SLOTS), lane)) ++n_issued;
-    cp_commit();
-    cp_wait<2>();
+    if (!bar_wait(&bars[slot], (uint32_t)((i / DW_SLOTS) & 1))) {
+      ok = false;  // a copy never landed: stop, report, leave C alone
+      if (lane == 0) atomicOr(&g_dw_err, 1u);
+      break;
+    }
     __syncwarp();
     const DPiece pc = ring[slot];
     const unsigned char *sbase = wsm + slot * DW_SLOT_BYTES;
@@ -566,6 +624,11 @@ __global__ void __launch_bounds__(DW_WARPS * 32, 1)
         if (row < pc.M && col < pc.N) pc.C[(long)row * pc.ldc + col] = acc[q];
       }
     }
+  }
+  if (!ok) {
+    // copies still in flight land before the CTA's shared memory goes away
+    for (long x = n_issued > DW_SLOTS ? n_issued - DW_SLOTS : 0; x < n_issued; ++x)
+      bar_wait(&bars[x % DW_SLOTS], (uint32_t)((x / DW_SLOTS) & 1));
   }
   cp_wait<0>();
 }
@@ -613,7 +676,18 @@ int run_dgemm_warp(const LibShalom_dgemm_entry *entries, long count, int method,
     }
   }
   if (rc) return rc;
-  return run_dgemm_runs_list(entries, count, pl.n_large, pl.large_first, pl.large_len);
+  rc = run_dgemm_runs_list(entries, count, pl.n_large, pl.large_first, pl.large_len);
+  if (rc || !st.sync) return rc;
+  // synchronous mode: report an expired wait on a staging barrier
+  unsigned err = 0;
+  LS_CUDA_TRY(cudaStreamSynchronize(st.stream));
+  LS_CUDA_TRY(cudaMemcpyFromSymbol(&err, g_dw_err, sizeof(err)));
+  if (err) {
+    const unsigned zero = 0;
+    LS_CUDA_TRY(cudaMemcpyToSymbol(g_dw_err, &zero, sizeof(zero)));
+    return LIBSHALOM_ERR_DEVICE_TIMEOUT;
+  }
+  return LIBSHALOM_SUCCESS;
 }
 
 }  // namespace ls
