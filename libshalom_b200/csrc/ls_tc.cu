@@ -1403,10 +1403,14 @@ __global__ void __launch_bounds__(G_THREADS, 1) k_tc_grouped(const GrpArgs g) {
         }
         const unsigned char *stg = smem + G_OFF_STAGE + st * G_STAGE_BYTES;
         unsigned char *base = smem + WS_OFF_BUF + b * BUF_BYTES;
+        // a last slab of at most 16 valid k takes one MMA k-step: its upper
+        // two 8-k chunks are never read, so they are not converted
+        const int nchunk = it.K - s * TC_BK <= 16 ? 2 : 4;
         if (cr < mrows) {
 #pragma unroll
           for (int q = 0; q < 2; ++q) {
             const int c = cc0 + 2 * q;
+            if (c >= nchunk) break;
             const unsigned char *row = stg + cr * 128;
             const float4 u0 = *reinterpret_cast<const float4 *>(row + (((2 * c) ^ (cr & 7)) << 4));
             const float4 u1 =
@@ -1424,7 +1428,7 @@ __global__ void __launch_bounds__(G_THREADS, 1) k_tc_grouped(const GrpArgs g) {
         for (int q = 0; q < 2; ++q) {
           const int e = ct + q * 256;
           const int jj = e % tn, c = e / tn;
-          if (e < 4 * tn && jj < ncols) {
+          if (e < 4 * tn && jj < ncols && c < nchunk) {
             float x[8];
             if (it.transb) {
               const unsigned char *row = stg + G_STAGE_A + jj * 128;
