@@ -11,12 +11,13 @@
 // Operand staging: every product is cut into K pieces (at most 32, fewer when
 // A and op(B) of 32 would not fit a slot), and the warp copies each piece into
 // one of three 8.5 KB per-warp slots, two pieces ahead of the one it
-// multiplies, with 16-byte cp.async only (any leading dimension, any 8-byte
-// alignment): an operand whose piece is one contiguous range (leading
-// dimension equal to the row length) is copied as the 16-byte aligned window
-// around that range; otherwise every row segment is copied as its own window
-// at a pitch of 16 (len/2 + 1) bytes.  Data starts 0 or 1 doubles into a
-// window (the address mod 16).  The description of every piece goes into a
+// multiplies (any leading dimension, any 8-byte alignment): an operand whose
+// piece is one contiguous range (leading dimension equal to the row length)
+// is copied as the 16-byte aligned window around that range by one bulk copy
+// (cp.async.bulk, its bytes counted on the slot's mbarrier); otherwise every
+// row segment is copied as its own window with 16-byte cp.async, at a pitch of
+// 16 (len/2 + 1) bytes.  Data starts 0 or 1 doubles into a window (the
+// address mod 16).  Waits on the slot barriers are bounded.  The description of every piece goes into a
 // per-warp ring next to the slots, so the entries, run table and pointer
 // arithmetic stay on the load side.
 //
