@@ -41,7 +41,7 @@ BATCH = 10_000
 METRIC = "batched small-GEMM GFLOP/s (cube sweep 8..128, NN+NT, 10,000 per size)"
 # DRAM bytes per algorithmic byte of the bf16x6 batched kernel, from one ncu
 # capture (profiles/k_tc_ws_bf16x6_nn128_batch2000.md)
-TRAFFIC_PER_ALG_BYTE = 0.897
+TRAFFIC_PER_ALG_BYTE = 0.910
 
 
 def step_flops(batch=BATCH):
@@ -419,7 +419,7 @@ def run_gpu(args):
         "roofline": {"bound": "hbm", "achieved": achieved_gbs, "peak": hbm_peak,
                      "unit": "GB/s", "frac": achieved_gbs / hbm_peak,
                      # DRAM bytes per launch: ncu dram__bytes_read + write of the same
-                     # kernel on a 2000-GEMM n=128 capture (0.897 per algorithmic byte,
+                     # kernel on a 2000-GEMM n=128 capture (0.910 per algorithmic byte,
                      # profiles/k_tc_ws_bf16x6_nn128_batch2000.md), scaled to the
                      # average launch of this sweep
                      "traffic": (TRAFFIC_PER_ALG_BYTE * step_bytes() / len(bufs)

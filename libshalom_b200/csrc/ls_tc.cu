@@ -28,6 +28,7 @@
 #include <cuda_bf16.h>
 
 #include <algorithm>
+#include <cstring>
 
 #include "ls_common.cuh"
 #include "ls_tc_launch.h"
@@ -564,17 +565,37 @@ done:
 //               accumulation chunk overlaps the MMAs of the next
 //   warps 2-9   converters: FP32 slab -> split BF16 core matrices (2 buffers)
 //   warps 10-17 epilogue: TMEM -> registers -> C (and the register fold of the
-//               long-K chunks)
+//               long-K chunks).  With beta = 0 and a TMA-addressable C (one
+//               GEMM per tile) each warp stages 32 rows x 32 columns of C in
+//               its own 4 KB shared buffer (128-byte swizzle) and writes them
+//               with one cp.async.bulk.tensor store: full-line writes instead
+//               of one 16-byte piece per row and thread, which would occupy the
+//               L1 data path the MMAs and converters share.
 // ===========================================================================
-constexpr int WS_WARPS = 18;
-constexpr int WS_THREADS = WS_WARPS * 32;
-constexpr int WS_STAGES = 4;
+constexpr int WS_STAGES = 3;
 constexpr int WS_STAGE_BYTES = 32768;                           // A 16 KB + B 16 KB
 constexpr int WS_OFF_BUF = 0;                                   // 2 BF16 operand buffers
 constexpr int WS_OFF_STAGE = 2 * BUF_BYTES;                     // 98304 (1024-aligned)
-constexpr int WS_OFF_BAR = WS_OFF_STAGE + WS_STAGES * WS_STAGE_BYTES;  // 229376
+constexpr int WS_CST_WARP = 4096;                               // C staging per epilogue warp
+constexpr int WS_OFF_CST = WS_OFF_STAGE + WS_STAGES * WS_STAGE_BYTES;  // 196608
+constexpr int WS_OFF_BAR = WS_OFF_CST + 8 * WS_CST_WARP;        // 229376
 constexpr int WS_SMEM = WS_OFF_BAR + 256;
-constexpr int W_CONV0 = 2, N_CONV = 8, W_EPI0 = 10, N_EPI = 8;
+static_assert(WS_SMEM <= 232448, "TMA kernel exceeds 227 KB of shared memory");
+constexpr int W_CONV0 = 2, N_CONV = 8;
+
+// Warp roles of k_tc_ws: warp 0 producer, warp 1 MMA, then NC converter and
+// NE epilogue warps.  WIDE (short K, C written by TMA stores): 16 converters
+// and 4 epilogue warps (one per TMEM lane quarter), since the split is the
+// busiest role there.  Otherwise 8 + 8: long-K tiles hold the register fold of
+// 64 columns per epilogue thread, and packed small GEMMs store C row by row.
+template <bool WIDE>
+struct WsRoles {
+  static constexpr int NC = WIDE ? 16 : 8;
+  static constexpr int NE = WIDE ? 4 : 8;
+  static constexpr int W_EPI = 2 + NC;
+  static constexpr int THREADS = (2 + NC + NE) * 32;
+  static constexpr int BLOCKS = 16 / NE;  // 32-column blocks of C per epilogue warp
+};
 constexpr int WS_TMEM_COLS = 512;  // 2 x (D_main 128 + D_corr 128)
 
 // mbarrier slots (8 bytes each) after WS_OFF_BAR
@@ -585,6 +606,7 @@ struct WsArgs {
   TcProblem p;
   uint32_t tx_bytes;  // A box + B box bytes per slab
   int nn_w;           // B (NoTrans) box width in floats (row pitch of the staged slab)
+  int c_tma;          // C written by TMA stores (boxes of 32 columns x 32 rows)
 };
 
 __device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
@@ -617,10 +639,10 @@ __device__ __forceinline__ bool ws_wait(uint64_t *bar, uint32_t parity, volatile
   return false;
 }
 
-template <int NSPLIT, bool DRAIN>
-__global__ void __launch_bounds__(WS_THREADS, 1)
+template <int NSPLIT, bool DRAIN, bool WIDE>
+__global__ void __launch_bounds__(WsRoles<WIDE>::THREADS, 1)
     k_tc_ws(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
-            const WsArgs args) {
+            const __grid_constant__ CUtensorMap tmC, const WsArgs args) {
   extern __shared__ __align__(1024) unsigned char smem[];
   const TcProblem &p = args.p;
   uint64_t *bars = reinterpret_cast<uint64_t *>(smem + WS_OFF_BAR);
@@ -630,17 +652,19 @@ __global__ void __launch_bounds__(WS_THREADS, 1)
   const uint32_t smem_base = ptx::smem_u32(smem);
   const int tn = p.tile_n;
   const int kc = DRAIN ? p.kc_slabs : (1 << 30);
+  static_assert(!(DRAIN && WIDE), "the long-K fold needs 8 epilogue warps");
+  using Roles = WsRoles<WIDE>;
 
   if (tid == 0) {
     for (int i = 0; i < WS_STAGES; ++i) {
       ptx::mbar_init(&bars[B_FULL + i], 1);
-      ptx::mbar_init(&bars[B_EMPTY + i], N_CONV);
+      ptx::mbar_init(&bars[B_EMPTY + i], Roles::NC);
     }
     for (int i = 0; i < 2; ++i) {
-      ptx::mbar_init(&bars[B_BFULL + i], N_CONV);
+      ptx::mbar_init(&bars[B_BFULL + i], Roles::NC);
       ptx::mbar_init(&bars[B_BEMPTY + i], 1);
       ptx::mbar_init(&bars[B_AFULL + i], 1);
-      ptx::mbar_init(&bars[B_AEMPTY + i], N_EPI);
+      ptx::mbar_init(&bars[B_AEMPTY + i], Roles::NE);
     }
     ptx::mbar_init(&bars[B_FINAL], 1);
     *s_abort = 0;
@@ -736,15 +760,25 @@ __global__ void __launch_bounds__(WS_THREADS, 1)
       ptx::mma_commit(&bars[B_FINAL]);
       ptx::mbar_wait_bounded(&bars[B_FINAL], 0);
     }
-  } else if (warp < W_EPI0) {
+  } else if (warp < Roles::W_EPI) {
     // ----------------------------- converters -----------------------------
-    const int ct = tid - W_CONV0 * 32;  // 0..255
-    const int cr = ct & 127, cc0 = ct >> 7;  // A rows cr, chunks cc0 and cc0 + 2
+    // items of a slab: A (row cr, 8-k chunk c) and B (column jj, chunk c),
+    // 512 of each, taken round-robin by the NCT threads (a fixed mapping:
+    // consecutive lanes take consecutive rows).  Rows and columns past the
+    // tile's GEMMs and the chunks past K of a last half slab are not
+    // converted: the MMA reads stale shared memory there, which reaches only
+    // output rows and columns that are never stored (and no MMA k-step at all).
+    constexpr int NCT = Roles::NC * 32;
+    constexpr int PER = 512 / NCT;
+    const int ct = tid - W_CONV0 * 32;
     const bool nn = !p.transb;
     const int nn_w = args.nn_w;
     long j = 0;
     bool ok = true;
     for (long t = blockIdx.x; ok && t < p.num_tiles; t += gridDim.x) {
+      const TileInfo ti = decode_tile(p, t);
+      const int a_rows = p.G > 1 ? ti.ng * p.M : min(TC_BM, p.M - ti.m0);
+      const int b_cols = p.G > 1 ? ti.ng * p.N : min(tn, p.N - ti.n0);
       for (int s = 0; s < p.nk; ++s, ++j) {
         const int st = (int)(j % WS_STAGES), b = (int)(j & 1);
         if (!ws_wait(&bars[B_FULL + st], (uint32_t)((j / WS_STAGES) & 1), s_abort, p.err)) {
@@ -756,29 +790,33 @@ __global__ void __launch_bounds__(WS_THREADS, 1)
           ok = false;
           break;
         }
+        const int nchunk = p.K - s * TC_BK <= 16 ? 2 : 4;  // the MMA's k-steps x 2
         const unsigned char *stg = smem + WS_OFF_STAGE + st * WS_STAGE_BYTES;
         unsigned char *base = smem + WS_OFF_BUF + b * BUF_BYTES;
 #pragma unroll
-        for (int q = 0; q < 2; ++q) {
-          // A: row cr, 8-float chunk c (16-byte chunks 2c, 2c+1, 128-byte swizzle)
-          const int c = cc0 + 2 * q;
-          const unsigned char *row = stg + cr * 128;
-          const float4 u0 = *reinterpret_cast<const float4 *>(row + (((2 * c) ^ (cr & 7)) << 4));
-          const float4 u1 =
-              *reinterpret_cast<const float4 *>(row + (((2 * c + 1) ^ (cr & 7)) << 4));
-          float x[8] = {u0.x, u0.y, u0.z, u0.w, u1.x, u1.y, u1.z, u1.w};
-          uint4 h, m, l;
-          split8<NSPLIT>(x, h, m, l);
-          const int off = c * CHUNK_BYTES + cr * 16;
-          *reinterpret_cast<uint4 *>(base + off) = h;
-          *reinterpret_cast<uint4 *>(base + SPLIT_BYTES + off) = m;
-          if (NSPLIT == 3) *reinterpret_cast<uint4 *>(base + 2 * SPLIT_BYTES + off) = l;
+        for (int q = 0; q < PER; ++q) {
+          const int idx = ct + q * NCT;
+          const int cr = idx & 127, c = idx >> 7;
+          if (cr < a_rows && c < nchunk) {
+            const unsigned char *row = stg + cr * 128;
+            const float4 u0 =
+                *reinterpret_cast<const float4 *>(row + (((2 * c) ^ (cr & 7)) << 4));
+            const float4 u1 =
+                *reinterpret_cast<const float4 *>(row + (((2 * c + 1) ^ (cr & 7)) << 4));
+            float x[8] = {u0.x, u0.y, u0.z, u0.w, u1.x, u1.y, u1.z, u1.w};
+            uint4 h, m, l;
+            split8<NSPLIT>(x, h, m, l);
+            const int off = c * CHUNK_BYTES + cr * 16;
+            *reinterpret_cast<uint4 *>(base + off) = h;
+            *reinterpret_cast<uint4 *>(base + SPLIT_BYTES + off) = m;
+            if (NSPLIT == 3) *reinterpret_cast<uint4 *>(base + 2 * SPLIT_BYTES + off) = l;
+          }
         }
 #pragma unroll
-        for (int q = 0; q < 2; ++q) {
-          const int e = ct + q * 256;
-          if (e < 4 * tn) {
-            const int jj = e % tn, c = e / tn;
+        for (int q = 0; q < PER; ++q) {
+          const int e = ct + q * NCT;
+          const int jj = e % tn, c = e / tn;
+          if (e < 4 * tn && jj < b_cols && c < nchunk) {
             float x[8];
             if (!nn) {
               const unsigned char *row = stg + 16384 + jj * 128;
@@ -790,19 +828,15 @@ __global__ void __launch_bounds__(WS_THREADS, 1)
               x[4] = u1.x; x[5] = u1.y; x[6] = u1.z; x[7] = u1.w;
             } else {
               // [g][32 k][nn_w] (packed) or [32 k][tn]: column jj of GEMM g = jj / N
-              // padding columns past the G packed GEMMs are not in the box: zero
               const float *fb = reinterpret_cast<const float *>(stg + 16384);
               int col = jj, gofs = 0;
-              bool in_box = true;
               if (p.G > 1) {
                 const int g = jj / p.N;
                 col = jj - g * p.N;
                 gofs = g * 32 * nn_w;
-                in_box = g < p.G;
               }
 #pragma unroll
-              for (int tk = 0; tk < 8; ++tk)
-                x[tk] = in_box ? fb[gofs + (8 * c + tk) * nn_w + col] : 0.0f;
+              for (int tk = 0; tk < 8; ++tk) x[tk] = fb[gofs + (8 * c + tk) * nn_w + col];
             }
             uint4 h, m, l;
             split8<NSPLIT>(x, h, m, l);
@@ -822,11 +856,23 @@ __global__ void __launch_bounds__(WS_THREADS, 1)
     }
   } else {
     // ------------------------------ epilogue ------------------------------
-    const int wq = warp & 3, half = (warp - W_EPI0) >> 2;
+    // warp (TMEM lane quarter wq, column group grp) owns the 32-column blocks
+    // grp, grp + NG, ... of its 32 rows: chunk q (8 columns) of the warp is
+    // tile chunk chunk_of(q)
+    constexpr int NG = Roles::NE / 4, BL = Roles::BLOCKS;
+    constexpr int NBUF = 8 / Roles::NE;  // 4 KB staging buffers per warp
+    const int ew = warp - Roles::W_EPI;
+    const int wq = warp & 3, grp = ew >> 2;
     const int r = wq * 32 + lane;
-    const int nch = tn / 8, per = (nch + 1) / 2;
-    const int c_begin = min(nch, half * per), c_end = min(nch, c_begin + per);
-    constexpr int RMAX = DRAIN ? 64 : 1;
+    const int nch = tn / 8;
+    auto chunk_of = [&](int q) { return 4 * (grp + NG * (q >> 2)) + (q & 3); };
+    int nb = 0;  // 32-column blocks of this warp inside the tile
+    while (nb < BL && chunk_of(4 * nb) < nch) ++nb;
+    const bool ctma = args.c_tma != 0;
+    unsigned char *cst = smem + WS_OFF_CST + ew * NBUF * WS_CST_WARP;
+    const uint32_t cst_u = smem_base + WS_OFF_CST + ew * NBUF * WS_CST_WARP;
+    int sb = 0;  // (lane 0) bulk stores issued by this warp
+    constexpr int RMAX = DRAIN ? 32 * BL : 1;
     float R[RMAX];
     long u = 0;
     bool ok = true;
@@ -877,6 +923,46 @@ __global__ void __launch_bounds__(WS_THREADS, 1)
           }
         }
       };
+      // block pb (chunks 4 pb .. 4 pb + 3 of the warp, values v[32]) of this
+      // warp's rows -> a staging buffer -> one TMA store; columns past tn are
+      // past N (the host requires tiles_n == 1 or tn % 32 == 0) and clipped
+      auto store_block = [&](int pb, const float *v) {
+        const int buf = NBUF > 1 ? (sb & 1) : 0;
+        if (lane == 0 && sb >= NBUF) {
+          if (NBUF > 1) ptx::bulk_wait_read<1>();  // the store that last used buf is done
+          else ptx::bulk_wait_read<0>();
+        }
+        __syncwarp();
+        unsigned char *row = cst + buf * WS_CST_WARP + lane * 128;
+#pragma unroll
+        for (int c = 0; c < 8; ++c) {
+          const float *x = v + 4 * c;
+          *reinterpret_cast<float4 *>(row + ((c ^ (lane & 7)) << 4)) =
+              make_float4(p.alpha * x[0], p.alpha * x[1], p.alpha * x[2], p.alpha * x[3]);
+        }
+        ptx::fence_proxy_async_smem();
+        __syncwarp();
+        if (lane == 0) {
+          ptx::tma_store_3d(&tmC, cst_u + buf * WS_CST_WARP, ti.n0 + chunk_of(4 * pb) * 8,
+                            ti.m0 + wq * 32, (int)ti.g0);
+          ptx::bulk_commit();
+        }
+        ++sb;
+      };
+      auto release = [&](int a) {
+        ptx::tc_fence_before();
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&bars[B_AEMPTY + a]);
+      };
+      const bool rows_in = ti.m0 + wq * 32 < p.M;  // G == 1 when ctma
+      // chunks holding columns of the GEMMs whose rows this warp covers
+      // (warp-uniform; every chunk for one GEMM per tile)
+      int c_lo = 0, c_hi = nch;
+      if (p.G > 1) {
+        const int g_lo = (wq * 32) / p.M, g_hi = min(ti.ng - 1, (wq * 32 + 31) / p.M);
+        c_lo = g_lo < ti.ng ? (g_lo * p.N) / 8 : nch;
+        c_hi = g_lo < ti.ng ? min(nch, ((g_hi + 1) * p.N + 7) / 8) : nch;
+      }
       const int nchunks = DRAIN ? (p.nk + kc - 1) / kc : 1;
 #pragma unroll
       for (int w = 0; w < RMAX; ++w) R[w] = 0.0f;
@@ -890,9 +976,9 @@ __global__ void __launch_bounds__(WS_THREADS, 1)
         const uint32_t acc_base = tmem + ((uint32_t)(wq * 32) << 16) + (uint32_t)(a * 256);
         if constexpr (DRAIN) {
 #pragma unroll
-          for (int q = 0; q < 8; ++q) {
-            const int ch = c_begin + q;
-            if (ch < c_end) {
+          for (int q = 0; q < 4 * BL; ++q) {
+            const int ch = chunk_of(q);
+            if (ch >= c_lo && ch < c_hi) {
               float dm[8], dc[8];
               ptx::tmem_ld8(acc_base + ch * 8, dm);
               ptx::tmem_ld8(acc_base + 128 + ch * 8, dc);
@@ -901,11 +987,38 @@ __global__ void __launch_bounds__(WS_THREADS, 1)
               for (int w = 0; w < 8; ++w) R[q * 8 + w] += dm[w] + dc[w];
             }
           }
-          ptx::tc_fence_before();
-          __syncwarp();
-          if (lane == 0) mbar_arrive(&bars[B_AEMPTY + a]);
+          release(a);
+        } else if (ctma) {
+          // block by block: TMEM loads, then (after the last block's loads)
+          // release the accumulator, then stage and store
+          if (nb == 0) release(a);
+#pragma unroll
+          for (int pb = 0; pb < BL; ++pb) {
+            if (pb < nb) {
+              float v[32];
+#pragma unroll
+              for (int q = 0; q < 4; ++q) {
+                const int ch = chunk_of(4 * pb + q);
+                float dc[8];
+                if (ch < nch) {
+                  ptx::tmem_ld8(acc_base + ch * 8, v + 8 * q);
+                  ptx::tmem_ld8(acc_base + 128 + ch * 8, dc);
+                } else {
+#pragma unroll
+                  for (int w = 0; w < 8; ++w) v[8 * q + w] = dc[w] = 0.0f;
+                }
+                ptx::tmem_wait_ld();
+#pragma unroll
+                for (int w = 0; w < 8; ++w) v[8 * q + w] += dc[w];
+              }
+              if (pb == nb - 1) release(a);
+              if (rows_in) store_block(pb, v);
+            }
+          }
         } else {
-          for (int ch = c_begin; ch < c_end; ++ch) {
+          for (int q = 0; q < 4 * BL; ++q) {
+            const int ch = chunk_of(q);
+            if (ch < c_lo || ch >= c_hi) continue;
             float dm[8], dc[8];
             ptx::tmem_ld8(acc_base + ch * 8, dm);
             ptx::tmem_ld8(acc_base + 128 + ch * 8, dc);
@@ -914,21 +1027,29 @@ __global__ void __launch_bounds__(WS_THREADS, 1)
             for (int w = 0; w < 8; ++w) dm[w] += dc[w];
             store8(ch, dm);
           }
-          ptx::tc_fence_before();
-          __syncwarp();
-          if (lane == 0) mbar_arrive(&bars[B_AEMPTY + a]);
+          release(a);
         }
       }
       if constexpr (DRAIN) {
         if (ok) {
+          if (ctma) {
+            if (rows_in) {
 #pragma unroll
-          for (int q = 0; q < 8; ++q) {
-            const int ch = c_begin + q;
-            if (ch < c_end) store8(ch, R + q * 8);
+              for (int pb = 0; pb < BL; ++pb)
+                if (pb < nb) store_block(pb, R + 32 * pb);
+            }
+          } else {
+#pragma unroll
+            for (int q = 0; q < 4 * BL; ++q) {
+              const int ch = chunk_of(q);
+              if (ch < nch) store8(ch, R + q * 8);
+            }
           }
         }
       }
     }
+    // the kernel's C writes are complete before the CTA exits
+    if (lane == 0 && sb > 0) ptx::bulk_wait_all();
   }
 
   __syncthreads();
@@ -1602,7 +1723,7 @@ bool encode_map(CUtensorMap *map, const float *base, uint64_t d0, uint64_t d1, u
 
 // Tensor maps for the warp-specialized kernel, or false when TMA cannot
 // address the operands (unaligned base or row stride, overlapping batches).
-bool ws_maps(const TcProblem &p, CUtensorMap *ma, CUtensorMap *mb, WsArgs *wa) {
+bool ws_maps(const TcProblem &p, CUtensorMap *ma, CUtensorMap *mb, CUtensorMap *mc, WsArgs *wa) {
   // split-K slices all read the one matrix pair: a single-batch tensor map
   const long count = p.kslice ? 1 : p.count;
   const long sA = count > 1 ? p.sA : (long)p.M * p.lda;
@@ -1632,6 +1753,15 @@ bool ws_maps(const TcProblem &p, CUtensorMap *ma, CUtensorMap *mb, WsArgs *wa) {
   wa->p = p;
   wa->tx_bytes = (uint32_t)(TC_BK * a1 * a2 + b0 * b1 * b2) * 4;
   wa->nn_w = p.transb ? 0 : (int)b0;
+  // C by TMA stores: beta = 0 (nothing to read), one GEMM per tile, 16-byte
+  // aligned rows, and every 32-column box either inside the tile or past N
+  wa->c_tma = 0;
+  const long sC = p.count > 1 ? p.sC : (long)p.M * p.ldc;
+  if (p.beta == 0.0f && p.G == 1 && aligned16(p.C) && p.ldc % 4 == 0 && sC % 4 == 0 &&
+      (p.count == 1 || sC >= (long)p.M * p.ldc) && (p.tiles_n == 1 || p.tile_n % 32 == 0) &&
+      encode_map(mc, p.C, p.N, p.M, p.count, (uint64_t)p.ldc * 4, (uint64_t)sC * 4, 32, 32, 1,
+                 true))
+    wa->c_tma = 1;
   return true;
 }
 
@@ -1653,16 +1783,24 @@ int tc_launch(TcProblem &p, int mode) {
   LS_CUDA_TRY(cudaGetSymbolAddress(&errp, g_tc_err));
   p.err = reinterpret_cast<unsigned *>(errp);
   const bool drain = p.nk > p.kc_slabs;
-  CUtensorMap ma, mb;
+  CUtensorMap ma, mb, mc;
+  memset(&mc, 0, sizeof(mc));
   WsArgs wa;
-  if (st.use_tma && ws_maps(p, &ma, &mb, &wa)) {
-    const void *kern = mode == LIBSHALOM_PREC_BF16X6
-                           ? (drain ? (const void *)k_tc_ws<3, true> : (const void *)k_tc_ws<3, false>)
-                           : (drain ? (const void *)k_tc_ws<2, true> : (const void *)k_tc_ws<2, false>);
-    (void)occupancy_of(kern, WS_THREADS, WS_SMEM, 1);  // raises the shared-memory limit
+  if (st.use_tma && ws_maps(p, &ma, &mb, &mc, &wa)) {
+    const bool wide = !drain && wa.c_tma;
+    const void *kern =
+        mode == LIBSHALOM_PREC_BF16X6
+            ? (drain  ? (const void *)k_tc_ws<3, true, false>
+               : wide ? (const void *)k_tc_ws<3, false, true>
+                      : (const void *)k_tc_ws<3, false, false>)
+            : (drain  ? (const void *)k_tc_ws<2, true, false>
+               : wide ? (const void *)k_tc_ws<2, false, true>
+                      : (const void *)k_tc_ws<2, false, false>);
+    const int threads = wide ? WsRoles<true>::THREADS : WsRoles<false>::THREADS;
+    (void)occupancy_of(kern, threads, WS_SMEM, 1);  // raises the shared-memory limit
     const int grid = grid_for(p.num_tiles, 1);
-    void *args[] = {&ma, &mb, &wa};
-    LS_CUDA_TRY(cudaLaunchKernel(kern, dim3(grid), dim3(WS_THREADS), args, WS_SMEM, st.stream));
+    void *args[] = {&ma, &mb, &mc, &wa};
+    LS_CUDA_TRY(cudaLaunchKernel(kern, dim3(grid), dim3(threads), args, WS_SMEM, st.stream));
   } else {
     const void *kern = mode == LIBSHALOM_PREC_BF16X6
                            ? (drain ? (const void *)k_tc_sgemm<3, true> : (const void *)k_tc_sgemm<3, false>)
