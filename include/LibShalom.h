@@ -197,6 +197,30 @@ LIBSHALOM_API int LibShalom_sgemm_batched_strided(int transb, long M, long N, lo
                                     const float *B, long strideB, float beta,
                                     float *C, long strideC, long count);
 
+/* Host-memory calls.  The reference's calls take HOST pointers; these do
+ * too (A, B and C in host memory; page-locked memory lets the copies run
+ * asynchronously), with the math, dispatch and status of the device-pointer
+ * calls of the same name.  The operands travel through a device staging
+ * buffer of three slots held by the library until LibShalom_finalize: the
+ * batched call is cut into chunks of whole GEMMs (about 64 MB of operands
+ * each) whose host-to-device copies, kernels and device-to-host copies
+ * overlap on three streams.  In asynchronous mode (LibShalom_set_sync(0))
+ * the call returns once everything is queued and the library's stream is
+ * ordered after the last copy back; the host buffers must stay valid until
+ * then.  The batched call needs strideC >= M * N when count > 1; beta != 0
+ * copies C in as well. */
+LIBSHALOM_API void LibShalom_sgemm_host(int transa, int transb, float *C, const float *A,
+                                        const float *B, long M, long N, long K);
+LIBSHALOM_API void LibShalom_sgemm_mp_host(int transa, int transb, float *C, const float *A,
+                                           const float *B, long M, long N, long K);
+LIBSHALOM_API void LibShalom_dgemm_host(int transa, int transb, double *C, const double *A,
+                                        const double *B, long M, long N, long K);
+LIBSHALOM_API int LibShalom_sgemm_batched_strided_host(int transb, long M, long N, long K,
+                                                       float alpha, const float *A,
+                                                       long strideA, const float *B,
+                                                       long strideB, float beta, float *C,
+                                                       long strideC, long count);
+
 /* Split-K SGEMM that allocates nothing.  No counterpart in the reference.
  * For callers that cannot allocate device memory (their GPU memory is owned
  * by another allocator, or a cudaMalloc in the middle of a call is not

@@ -55,6 +55,8 @@ EXPORTED = (
     "LibShalom_finalize",
     "LibShalom_sgemm_batched", "LibShalom_sgemm_batched_strided",
     "LibShalom_dgemm_batched", "LibShalom_sgemm_mp_noalloc",
+    "LibShalom_sgemm_host", "LibShalom_sgemm_mp_host", "LibShalom_dgemm_host",
+    "LibShalom_sgemm_batched_strided_host",
 )
 
 _L = ctypes.c_long
@@ -118,6 +120,11 @@ _SIGS = {
                                              _L]),
     "LibShalom_dgemm_batched": (_I, [_P, _L]),
     "LibShalom_sgemm_mp_noalloc": (_I, [_I, _I, _P, _P, _P, _L, _L, _L, _I]),
+    "LibShalom_sgemm_host": (None, [_I, _I, _P, _P, _P, _L, _L, _L]),
+    "LibShalom_sgemm_mp_host": (None, [_I, _I, _P, _P, _P, _L, _L, _L]),
+    "LibShalom_dgemm_host": (None, [_I, _I, _P, _P, _P, _L, _L, _L]),
+    "LibShalom_sgemm_batched_strided_host": (_I, [_I, _L, _L, _L, _F, _P, _L, _P, _L, _F, _P,
+                                                  _L, _L]),
 }
 
 _lib = None
@@ -161,6 +168,17 @@ def _ptr(x) -> int | None:
     return x.data_ptr()
 
 
+def _hptr(x) -> int | None:
+    """Host address of a numpy array or a CPU torch tensor (or an int)."""
+    if x is None or isinstance(x, int):
+        return x
+    if hasattr(x, "ctypes"):
+        return x.ctypes.data
+    if getattr(x, "is_cuda", False):
+        raise ValueError("host-memory call given a CUDA tensor")
+    return x.data_ptr()
+
+
 def _check(status: int, what: str) -> None:
     if status != SUCCESS:
         raise LibShalomError(status, what)
@@ -191,6 +209,31 @@ def dgemm(transa, transb, C, A, B, M, N, K, check=True) -> int:
     st = last_error()
     if check:
         _check(st, "LibShalom_dgemm")
+    return st
+
+
+def sgemm_host(transa, transb, C, A, B, M, N, K, check=True) -> int:
+    """LibShalom_sgemm with A, B and C in host memory (numpy / CPU tensors)."""
+    lib().LibShalom_sgemm_host(transa, transb, _hptr(C), _hptr(A), _hptr(B), M, N, K)
+    st = last_error()
+    if check:
+        _check(st, "LibShalom_sgemm_host")
+    return st
+
+
+def sgemm_mp_host(transa, transb, C, A, B, M, N, K, check=True) -> int:
+    lib().LibShalom_sgemm_mp_host(transa, transb, _hptr(C), _hptr(A), _hptr(B), M, N, K)
+    st = last_error()
+    if check:
+        _check(st, "LibShalom_sgemm_mp_host")
+    return st
+
+
+def dgemm_host(transa, transb, C, A, B, M, N, K, check=True) -> int:
+    lib().LibShalom_dgemm_host(transa, transb, _hptr(C), _hptr(A), _hptr(B), M, N, K)
+    st = last_error()
+    if check:
+        _check(st, "LibShalom_dgemm_host")
     return st
 
 
@@ -343,6 +386,18 @@ def sgemm_batched_strided(transb, M, N, K, alpha, A, strideA, B, strideB, beta, 
                                                _ptr(B), strideB, beta, _ptr(C), strideC, count)
     if check:
         _check(st, "LibShalom_sgemm_batched_strided")
+    return st
+
+
+def sgemm_batched_strided_host(transb, M, N, K, alpha, A, strideA, B, strideB, beta, C,
+                               strideC, count, check=True) -> int:
+    """Uniform batch with A, B and C in host memory (copies pipelined with the
+    kernels; page-locked memory makes them asynchronous)."""
+    st = lib().LibShalom_sgemm_batched_strided_host(transb, M, N, K, alpha, _hptr(A), strideA,
+                                                    _hptr(B), strideB, beta, _hptr(C), strideC,
+                                                    count)
+    if check:
+        _check(st, "LibShalom_sgemm_batched_strided_host")
     return st
 
 

@@ -317,6 +317,169 @@ static int gemm_cached(int kind, int transa, int transb, T *C, const T *A, const
 
 }  // namespace ls
 
+// ---------------------------------------------------------------------------
+// Host-memory calls.  The reference's API takes host pointers; these entry
+// points do too.  Operands go through a device staging buffer of three slots:
+// a call is cut into chunks of whole GEMMs that rotate over the slots, with
+// the host->device copies on one stream, the kernels on the library's stream
+// and the device->host copies on a third, ordered by per-slot events.  Both
+// copy directions and the kernels of neighbouring chunks (and of consecutive
+// calls) overlap; page-locked host memory makes the copies asynchronous.
+// ---------------------------------------------------------------------------
+namespace ls {
+
+static constexpr size_t HS_CHUNK_BYTES = 64u << 20;  // target operand bytes per chunk
+
+static void host_staging_release() {
+  State &st = state();
+  if (st.hs_in) cudaStreamSynchronize(st.hs_in);
+  if (st.hs_out) cudaStreamSynchronize(st.hs_out);
+  if (st.hs) cudaFree(st.hs);
+  for (int i = 0; i < 3; ++i) {
+    if (st.hs_ev_in[i]) cudaEventDestroy(st.hs_ev_in[i]);
+    if (st.hs_ev_done[i]) cudaEventDestroy(st.hs_ev_done[i]);
+    if (st.hs_ev_out[i]) cudaEventDestroy(st.hs_ev_out[i]);
+    st.hs_ev_in[i] = st.hs_ev_done[i] = st.hs_ev_out[i] = nullptr;
+  }
+  if (st.hs_in) cudaStreamDestroy(st.hs_in);
+  if (st.hs_out) cudaStreamDestroy(st.hs_out);
+  st.hs_in = st.hs_out = nullptr;
+  st.hs = nullptr;
+  st.hs_slot_bytes = 0;
+  st.hs_device = -1;
+}
+
+// Staging slots of at least slot_bytes each, the copy streams and events of
+// the current device.
+static int host_staging(size_t slot_bytes) {
+  State &st = state();
+  if (st.hs_device != st.device) {
+    if (st.hs_device >= 0) {
+      // the staging of another device: finish its work and drop it
+      int cur = st.device;
+      cudaSetDevice(st.hs_device);
+      host_staging_release();
+      cudaSetDevice(cur);
+    }
+    LS_CUDA_TRY(cudaStreamCreateWithFlags(&st.hs_in, cudaStreamNonBlocking));
+    LS_CUDA_TRY(cudaStreamCreateWithFlags(&st.hs_out, cudaStreamNonBlocking));
+    for (int i = 0; i < 3; ++i) {
+      LS_CUDA_TRY(cudaEventCreateWithFlags(&st.hs_ev_in[i], cudaEventDisableTiming));
+      LS_CUDA_TRY(cudaEventCreateWithFlags(&st.hs_ev_done[i], cudaEventDisableTiming));
+      LS_CUDA_TRY(cudaEventCreateWithFlags(&st.hs_ev_out[i], cudaEventDisableTiming));
+    }
+    st.hs_device = st.device;
+  }
+  if (st.hs && st.hs_slot_bytes >= slot_bytes) return LIBSHALOM_SUCCESS;
+  if (st.hs) {
+    // copies and kernels queued earlier may still use the old slots
+    LS_CUDA_TRY(cudaStreamSynchronize(st.hs_in));
+    LS_CUDA_TRY(cudaStreamSynchronize(st.stream));
+    LS_CUDA_TRY(cudaStreamSynchronize(st.hs_out));
+    cudaFree(st.hs);
+    st.hs = nullptr;
+    st.hs_slot_bytes = 0;
+  }
+  const size_t want = (std::max(slot_bytes, (size_t)1 << 20) + 255) / 256 * 256;
+  if (cudaMalloc(&st.hs, 3 * want) != cudaSuccess) {
+    cudaGetLastError();
+    st.hs = nullptr;
+    return LIBSHALOM_ERR_ALLOC;
+  }
+  st.hs_slot_bytes = want;
+  return LIBSHALOM_SUCCESS;
+}
+
+// elements a chunk of n matrices of `elems` elements at host stride `stride`
+// occupies in a slot: the host span itself when matrices overlap or touch
+// (stride <= elems, device stride = stride), else packed (device stride = elems)
+static long staged_elems(long n, long elems, long stride) {
+  if (elems == 0 || n == 0) return 0;
+  return stride <= elems ? (n - 1) * stride + elems : n * elems;
+}
+static long staged_stride(long elems, long stride) { return stride <= elems ? stride : elems; }
+
+template <typename T>
+static int copy_in(T *dst, const T *src, long n, long elems, long stride, cudaStream_t s) {
+  if (elems == 0 || n == 0) return LIBSHALOM_SUCCESS;
+  if (stride <= elems) {
+    LS_CUDA_TRY(cudaMemcpyAsync(dst, src, sizeof(T) * staged_elems(n, elems, stride),
+                                cudaMemcpyHostToDevice, s));
+  } else {
+    LS_CUDA_TRY(cudaMemcpy2DAsync(dst, sizeof(T) * elems, src, sizeof(T) * stride,
+                                  sizeof(T) * elems, n, cudaMemcpyHostToDevice, s));
+  }
+  return LIBSHALOM_SUCCESS;
+}
+
+static size_t align256(size_t b) { return (b + 255) / 256 * 256; }
+
+// count GEMMs (matrix g of A at A + g * sA, ...) through the staging slots;
+// compute(dA, dB, dC, dsA, dsB, dsC, g0, n) launches the kernels of GEMMs
+// g0 .. g0 + n - 1 on the library's stream.  C (elems_c per GEMM) must not
+// overlap between GEMMs; it is copied in only when c_in.
+template <typename T, typename Compute>
+static int host_pipeline(long count, long elems_a, long sA, const T *A, long elems_b, long sB,
+                         const T *B, long elems_c, long sC, T *C, bool c_in, Compute compute) {
+  State &st = state();
+  const size_t per = sizeof(T) * (size_t)(elems_a + elems_b + elems_c);
+  const long cc = std::max(1L, std::min(count, (long)(HS_CHUNK_BYTES / std::max(per, (size_t)1))));
+  const size_t off_b = align256(sizeof(T) * staged_elems(cc, elems_a, sA));
+  const size_t off_c = off_b + align256(sizeof(T) * staged_elems(cc, elems_b, sB));
+  const size_t slot = off_c + align256(sizeof(T) * (size_t)cc * elems_c);
+  int rc = host_staging(slot);
+  if (rc) return rc;
+  const long dsA = staged_stride(elems_a, sA), dsB = staged_stride(elems_b, sB);
+  int last = -1;
+  for (long g0 = 0; g0 < count; g0 += cc) {
+    const long n = std::min(cc, count - g0);
+    const int s = (int)(st.hs_next++ % 3);
+    unsigned char *base = static_cast<unsigned char *>(st.hs) + (size_t)s * st.hs_slot_bytes;
+    T *dA = reinterpret_cast<T *>(base), *dB = reinterpret_cast<T *>(base + off_b);
+    T *dC = reinterpret_cast<T *>(base + off_c);
+    // the slot's previous chunk has been computed and copied out
+    LS_CUDA_TRY(cudaStreamWaitEvent(st.hs_in, st.hs_ev_out[s], 0));
+    if ((rc = copy_in(dA, A + g0 * sA, n, elems_a, sA, st.hs_in))) return rc;
+    if ((rc = copy_in(dB, B + g0 * sB, n, elems_b, sB, st.hs_in))) return rc;
+    if (c_in && (rc = copy_in(dC, C + g0 * sC, n, elems_c, sC, st.hs_in))) return rc;
+    LS_CUDA_TRY(cudaEventRecord(st.hs_ev_in[s], st.hs_in));
+    LS_CUDA_TRY(cudaStreamWaitEvent(st.stream, st.hs_ev_in[s], 0));
+    if ((rc = compute(dA, dB, dC, dsA, dsB, elems_c, g0, n))) return rc;
+    LS_CUDA_TRY(cudaEventRecord(st.hs_ev_done[s], st.stream));
+    LS_CUDA_TRY(cudaStreamWaitEvent(st.hs_out, st.hs_ev_done[s], 0));
+    if (sC == elems_c || n == 1)
+      LS_CUDA_TRY(cudaMemcpyAsync(C + g0 * sC, dC, sizeof(T) * (size_t)n * elems_c,
+                                  cudaMemcpyDeviceToHost, st.hs_out));
+    else
+      LS_CUDA_TRY(cudaMemcpy2DAsync(C + g0 * sC, sizeof(T) * sC, dC, sizeof(T) * elems_c,
+                                    sizeof(T) * elems_c, n, cudaMemcpyDeviceToHost,
+                                    st.hs_out));
+    LS_CUDA_TRY(cudaEventRecord(st.hs_ev_out[s], st.hs_out));
+    last = s;
+  }
+  // the caller's stream is ordered after the last copy out
+  if (last >= 0) LS_CUDA_TRY(cudaStreamWaitEvent(st.stream, st.hs_ev_out[last], 0));
+  return finish_launch("host pipeline");
+}
+
+template <typename T>
+static int gemm_host(int transa, int transb, T *C, const T *A, const T *B, long M, long N,
+                     long K, bool mp) {
+  if ((transa != NoTrans && transa != Trans) || (transb != NoTrans && transb != Trans) ||
+      M < 0 || N < 0 || K < 0)
+    return LIBSHALOM_ERR_INVALID_VALUE;
+  if (M == 0 || N == 0) return LIBSHALOM_SUCCESS;
+  if (!C || (K > 0 && (!A || !B))) return LIBSHALOM_ERR_INVALID_VALUE;
+  int rc = ensure_device();
+  if (rc) return rc;
+  auto compute = [&](T *dA, T *dB, T *dC, long, long, long, long, long) {
+    return gemm_common<T>(transa, transb, dC, dA, dB, M, N, K, mp);
+  };
+  return host_pipeline<T>(1, M * K, M * K, A, K * N, K * N, B, M * N, M * N, C, false, compute);
+}
+
+}  // namespace ls
+
 using namespace ls;
 
 extern "C" {
@@ -480,6 +643,13 @@ void LibShalom_finalize(void) {
   State &st = state();
   if (st.ws || st.fe) cudaStreamSynchronize(st.stream);
   graph_cache_clear();
+  if (st.hs_device >= 0) {
+    int cur = -1;
+    cudaGetDevice(&cur);
+    cudaSetDevice(st.hs_device);
+    host_staging_release();
+    if (cur >= 0) cudaSetDevice(cur);
+  }
   if (st.ws) cudaFree(st.ws);
   if (st.fe) cudaFree(st.fe);
   st.ws = nullptr;
@@ -533,6 +703,65 @@ int LibShalom_sgemm_batched_strided(int transb, long M, long N, long K, float al
   }
   set_error(rc);
   return rc;
+}
+
+int LibShalom_sgemm_batched_strided_host(int transb, long M, long N, long K, float alpha,
+                                         const float *A, long strideA, const float *B,
+                                         long strideB, float beta, float *C, long strideC,
+                                         long count) {
+  std::lock_guard<std::mutex> lk(state().mu);
+  int rc = LIBSHALOM_SUCCESS;
+  if ((transb != NoTrans && transb != Trans) || M < 0 || N < 0 || K < 0 || count < 0 ||
+      strideA < 0 || strideB < 0 || strideC < 0)
+    rc = LIBSHALOM_ERR_INVALID_VALUE;
+  else if (count > 1 && strideC < M * N)
+    rc = LIBSHALOM_ERR_INVALID_VALUE;  // the copies out would overlap
+  else if (count > 0 && M > 0 && N > 0 && (!C || (K > 0 && (!A || !B))))
+    rc = LIBSHALOM_ERR_INVALID_VALUE;
+  else if (count > 0 && M > 0 && N > 0 && !(rc = ensure_device())) {
+    const int prec = state().precision;
+    auto compute = [&](float *dA, float *dB, float *dC, long dsA, long dsB, long dsC, long,
+                       long n) {
+      GemmArgs<float> g;
+      g.A = dA; g.B = dB; g.C = dC;
+      g.M = M; g.N = N; g.K = K;
+      g.transa = 0; g.transb = transb;
+      g.lda = K; g.ldb = transb ? K : N; g.ldc = N;
+      g.alpha = alpha; g.beta = beta;
+      const int r = prec == LIBSHALOM_PREC_FP32
+                        ? run_strided<float>(g, dsA, dsB, dsC, n)
+                        : tc_sgemm_strided(g, dsA, dsB, dsC, n, prec);
+      if (r) return r;
+      const cudaError_t e = cudaGetLastError();
+      if (e != cudaSuccess) {
+        note_cuda_error(e, "sgemm_batched_strided_host", __FILE__, __LINE__);
+        return (int)LIBSHALOM_ERR_CUDA;
+      }
+      return (int)LIBSHALOM_SUCCESS;
+    };
+    rc = host_pipeline<float>(count, M * K, strideA, A, K * N, strideB, B, M * N,
+                              count > 1 ? strideC : M * N, C, beta != 0.0f, compute);
+  }
+  set_error(rc);
+  return rc;
+}
+
+void LibShalom_sgemm_host(int transa, int transb, float *C, const float *A, const float *B,
+                          long M, long N, long K) {
+  std::lock_guard<std::mutex> lk(state().mu);
+  set_error(gemm_host<float>(transa, transb, C, A, B, M, N, K, false));
+}
+
+void LibShalom_sgemm_mp_host(int transa, int transb, float *C, const float *A, const float *B,
+                             long M, long N, long K) {
+  std::lock_guard<std::mutex> lk(state().mu);
+  set_error(gemm_host<float>(transa, transb, C, A, B, M, N, K, true));
+}
+
+void LibShalom_dgemm_host(int transa, int transb, double *C, const double *A, const double *B,
+                          long M, long N, long K) {
+  std::lock_guard<std::mutex> lk(state().mu);
+  set_error(gemm_host<double>(transa, transb, C, A, B, M, N, K, false));
 }
 
 int LibShalom_dgemm_batched(const LibShalom_dgemm_entry *entries, long count) {

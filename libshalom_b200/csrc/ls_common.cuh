@@ -64,6 +64,14 @@ struct State {
   int fe_device = -1;
   unsigned ws_generation = 0;  // bumped whenever the workspace moves
   int graph_cache = 0;         // replay repeated identical single / mp calls
+  // host-memory calls: device staging of three slots, the two copy streams
+  // and, per slot, the events "inputs copied", "computed", "output copied"
+  void *hs = nullptr;
+  size_t hs_slot_bytes = 0;
+  int hs_device = -1;
+  cudaStream_t hs_in = nullptr, hs_out = nullptr;
+  cudaEvent_t hs_ev_in[3] = {}, hs_ev_done[3] = {}, hs_ev_out[3] = {};
+  unsigned hs_next = 0;
 };
 
 State &state();
