@@ -77,6 +77,30 @@ def test_tc_ragged(M, N, K, transb, mode_setter, staging):
         _check(C[g], A[g], B[g], transb, ls.PREC_BF16X6)
 
 
+@pytest.mark.parametrize("transb", [0, 1])
+@pytest.mark.parametrize("M,N,K", [(8, 8, 8), (12, 20, 24), (24, 24, 24), (20, 60, 33),
+                                   (40, 40, 40), (56, 56, 56), (64, 64, 64), (60, 64, 17),
+                                   (16, 52, 70), (13, 9, 33), (72, 72, 72), (130, 100, 64)])
+def test_tc_batch_every_gemm_and_nothing_past_c(M, N, K, transb, mode_setter):
+    """Every GEMM of a batch whose count leaves a partial last tile (packed
+    small GEMMs with row stores; one GEMM per tile with C by TMA boxes), and
+    the floats after the batch's C stay as they were."""
+    import torch
+    count = 53
+    A = orc.uniform_f32(M + N + K, count * M * K).reshape(count, M, K)
+    B = orc.uniform_f32(M + N + K + 1, count * K * N).reshape((count, N, K) if transb
+                                                              else (count, K, N))
+    buf = torch.full((count * M * N + 256,), 7.0, device="cuda")
+    ls.set_precision(ls.PREC_BF16X6)
+    ls.sgemm_batched_strided(transb, M, N, K, 1.0, to_dev(A), M * K, to_dev(B), K * N, 0.0,
+                             buf, M * N, count)
+    h = to_host(buf)
+    assert np.all(h[count * M * N:] == 7.0)
+    C = h[:count * M * N].reshape(count, M, N)
+    for g in range(count):
+        _check(C[g], A[g], B[g], transb, ls.PREC_BF16X6)
+
+
 def test_tc_alpha_beta(mode_setter):
     A, B, C0, C = _strided(ls.PREC_BF16X6, 1, 24, 40, 56, 20, seed=5, alpha=-0.5, beta=1.0)
     for g in range(20):
