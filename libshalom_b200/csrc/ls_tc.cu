@@ -1182,8 +1182,10 @@ constexpr int G_SMEM = G_OFF_Q + GQ * (int)sizeof(GSlot);
 static_assert(G_SMEM <= 232448, "grouped kernel exceeds 227 KB of shared memory");
 
 // warp 0 MMA, 1 scheduler, 2-9 converters (which also stage the operands),
-// 10-25 epilogue (4 TMEM lane quarters x 4 column quarters: 32 columns of one
-// row a thread)
+// 10-25 epilogue.  The MMAs compute C^T (op(B)^T as the 128-row operand, A as
+// the N operand): TMEM lanes are the tile's columns, so the 16 epilogue warps
+// (4 TMEM lane quarters x 4 row quarters) hold one column and up to 32 rows a
+// thread and read / write C one row of 32 consecutive floats per instruction.
 constexpr int G_W_MMA = 0, G_W_SCHED = 1, G_W_CONV0 = 2, G_W_EPI0 = 10;
 constexpr int G_N_EPI = 16;
 constexpr int G_WARPS = 26;
@@ -1380,7 +1382,10 @@ __global__ void __launch_bounds__(G_THREADS, 1) k_tc_grouped(const GrpArgs g) {
         GItem it;
         if (!q_get(smem, j, it, s_abort, g.err)) break;
         if (it.M < 0) break;
-        const uint32_t idesc = ptx::idesc_bf16_f32(TC_BM, it.tn);
+        // C^T = op(B)^T A^T: the 128 MMA rows (TMEM lanes) are the tile's
+        // columns, the MMA N its rows (rounded to 16)
+        const int mrows = min(TC_BM, it.M - it.m0);
+        const uint32_t idesc = ptx::idesc_bf16_f32(TC_BM, (mrows + 15) / 16 * 16);
         for (int s = 0; s < it.nk; ++s, ++js) {
           const int s_in = s % kc;
           if (s_in == 0) {
@@ -1404,12 +1409,12 @@ __global__ void __launch_bounds__(G_THREADS, 1) k_tc_grouped(const GrpArgs g) {
           for (int ks = 0; ks < 2; ++ks) {
             if (ks >= ksteps) break;
             const uint32_t acc = (s_in > 0 || ks > 0) ? 1u : 0u;
-            uint64_t da[3], db[3];
+            uint64_t da[3], db[3];  // da: op(B) columns (MMA rows), db: A rows
 #pragma unroll
             for (int sp = 0; sp < NSPLIT; ++sp) {
-              da[sp] = ptx::smem_desc(bb + sp * SPLIT_BYTES + ks * 2 * CHUNK_BYTES, CHUNK_BYTES, 128);
-              db[sp] = ptx::smem_desc(bb + sp * SPLIT_BYTES + 8192 + ks * 2 * CHUNK_BYTES,
+              da[sp] = ptx::smem_desc(bb + sp * SPLIT_BYTES + 8192 + ks * 2 * CHUNK_BYTES,
                                       CHUNK_BYTES, 128);
+              db[sp] = ptx::smem_desc(bb + sp * SPLIT_BYTES + ks * 2 * CHUNK_BYTES, CHUNK_BYTES, 128);
             }
             ptx::mma_bf16(acc_base, da[0], db[0], idesc, acc);
             ptx::mma_bf16(acc_base + 128, da[0], db[1], idesc, acc);
@@ -1583,45 +1588,33 @@ __global__ void __launch_bounds__(G_THREADS, 1) k_tc_grouped(const GrpArgs g) {
     cp_async_wait<0>();
   } else {
     // ------------------------------ epilogue ------------------------------
-    // The thread's C segment (one row, up to 32 columns) is loaded into R
-    // before the accumulator is ready, so those loads overlap the MMAs; each
-    // TMEM chunk is folded into R (the first as alpha*D + beta*C, later K
-    // chunks as R + alpha*D) and released at once; R is stored at the end.
+    // The accumulator holds C^T: TMEM lane = tile column, TMEM column = tile
+    // row.  Thread (lane quarter wq, lane) owns column n0 + 32 wq + lane and
+    // up to 32 rows (4 chunks of 8) of its warp's row quarter, so every beta
+    // load and every store of one row is 32 consecutive floats across the
+    // warp, whatever the alignment of C.  Each TMEM chunk is added into R as
+    // alpha*D and released at once; at the end C = beta*C + R, eight rows at
+    // a time (their loads issued together).
     const int wq = warp & 3, quarter = (warp - G_W_EPI0) >> 2;
-    const int r = wq * 32 + lane;
+    const int jc = wq * 32 + lane;  // tile column of this thread
     long u = 0;
     bool ok = true;
     for (long j = 0; ok; ++j) {
       GItem it;
       if (!q_get(smem, j, it, s_abort, g.err)) break;
       if (it.M < 0) break;
-      const int tn = it.tn, nch = tn / 8, per = (nch + 3) / 4;
-      const int c_begin = min(nch, quarter * per), c_end = min(nch, c_begin + per);
-      const int i = it.m0 + r;
-      const bool rok = i < it.M;
-      const int jhi = min(tn, it.N - it.n0);
-      float *crow = it.C + (long)i * it.ldc + it.n0;
-      const bool vec = ((reinterpret_cast<uintptr_t>(it.C) & 15) == 0) && (it.ldc & 3) == 0;
-      const bool rd = rok && it.beta != 0.0f;
+      const int mrows = min(TC_BM, it.M - it.m0);
+      const int nchr = (mrows + 15) / 16 * 2, per = (nchr + 3) / 4;  // chunks of 8 rows
+      const int c_begin = min(nchr, quarter * per), c_end = min(nchr, c_begin + per);
+      const bool cok = jc < min(it.tn, it.N - it.n0);
+      // this thread's rows: i0 .. i0 + n_rows - 1, at C[m0 + i][n0 + jc]
+      const int i0 = c_begin * 8, n_rows = max(0, min(mrows, c_end * 8) - i0);
+      const long ld = it.ldc;
+      float *c0 = it.C + (long)(it.m0 + i0) * ld + it.n0 + jc;
+      const bool rd = cok && it.beta != 0.0f;
       float R[32];
 #pragma unroll
-      for (int q = 0; q < 4; ++q) {
-        const int j0 = (c_begin + q) * 8;
-        if (rd && c_begin + q < c_end && j0 < jhi) {
-          if (vec && j0 + 8 <= jhi) {
-            const float4 c0 = *reinterpret_cast<const float4 *>(crow + j0);
-            const float4 c1 = *reinterpret_cast<const float4 *>(crow + j0 + 4);
-            R[q * 8 + 0] = c0.x; R[q * 8 + 1] = c0.y; R[q * 8 + 2] = c0.z; R[q * 8 + 3] = c0.w;
-            R[q * 8 + 4] = c1.x; R[q * 8 + 5] = c1.y; R[q * 8 + 6] = c1.z; R[q * 8 + 7] = c1.w;
-          } else {
-#pragma unroll
-            for (int w = 0; w < 8; ++w) R[q * 8 + w] = j0 + w < jhi ? crow[j0 + w] : 0.0f;
-          }
-        } else {
-#pragma unroll
-          for (int w = 0; w < 8; ++w) R[q * 8 + w] = 0.0f;
-        }
-      }
+      for (int t = 0; t < 32; ++t) R[t] = 0.0f;
       const int nchunks = (it.nk + kc - 1) / kc;
       for (int cu = 0; cu < nchunks; ++cu, ++u) {
         const int a = (int)(u & 1);
@@ -1631,7 +1624,6 @@ __global__ void __launch_bounds__(G_THREADS, 1) k_tc_grouped(const GrpArgs g) {
         }
         ptx::tc_fence_after();
         const uint32_t acc_base = tmem + ((uint32_t)(wq * 32) << 16) + (uint32_t)(a * 256);
-        const float cb = cu == 0 ? (rd ? it.beta : 0.0f) : 1.0f;
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
           if (c_begin + q < c_end) {
@@ -1642,9 +1634,7 @@ __global__ void __launch_bounds__(G_THREADS, 1) k_tc_grouped(const GrpArgs g) {
               ptx::tmem_ld4(acc_base + 128 + (c_begin + q) * 8 + 4 * h, dc);
               ptx::tmem_wait_ld();
 #pragma unroll
-              for (int w = 0; w < 4; ++w)
-                R[q * 8 + 4 * h + w] =
-                    __fmaf_rn(cb, R[q * 8 + 4 * h + w], it.alpha * (dm[w] + dc[w]));
+              for (int w = 0; w < 4; ++w) R[q * 8 + 4 * h + w] += it.alpha * (dm[w] + dc[w]);
             }
           }
         }
@@ -1654,20 +1644,21 @@ __global__ void __launch_bounds__(G_THREADS, 1) k_tc_grouped(const GrpArgs g) {
       }
       __syncwarp();
       if (ok && lane == 0) mbar_arrive(&qempty[j % GQ]);
-      if (!ok || !rok) continue;
+      if (!ok || !cok) continue;
+      {
+        float *pc = c0;
 #pragma unroll
-      for (int q = 0; q < 4; ++q) {
-        const int j0 = (c_begin + q) * 8;
-        if (c_begin + q >= c_end || j0 >= jhi) continue;
-        if (vec && j0 + 8 <= jhi) {
-          *reinterpret_cast<float4 *>(crow + j0) =
-              make_float4(R[q * 8 + 0], R[q * 8 + 1], R[q * 8 + 2], R[q * 8 + 3]);
-          *reinterpret_cast<float4 *>(crow + j0 + 4) =
-              make_float4(R[q * 8 + 4], R[q * 8 + 5], R[q * 8 + 6], R[q * 8 + 7]);
-        } else {
+        for (int g8 = 0; g8 < 4; ++g8) {
+          float cv[8];
 #pragma unroll
           for (int w = 0; w < 8; ++w)
-            if (j0 + w < jhi) crow[j0 + w] = R[q * 8 + w];
+            cv[w] = rd && g8 * 8 + w < n_rows ? pc[(long)w * ld] : 0.0f;
+#pragma unroll
+          for (int w = 0; w < 8; ++w) {
+            const int t = g8 * 8 + w;
+            if (t < n_rows) pc[(long)w * ld] = rd ? __fmaf_rn(it.beta, cv[w], R[t]) : R[t];
+          }
+          pc += 8 * ld;
         }
       }
     }
