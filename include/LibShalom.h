@@ -281,9 +281,12 @@ LIBSHALOM_API int LibShalom_dgemm_stack(const LibShalom_dgemm_stack_desc *stack,
  * benchmark feeds LibShalom_sgemm_mp with im2col shapes): FP32 NCHW
  * cross-correlation, x [n][c][h][w], weights [oc][c][kh][kw], y [n][oc][oh][ow]
  * with oh = (h + 2 ph - kh) / sh + 1, ow = (w + 2 pw - kw) / sw + 1, zero
- * padding; each image is expanded by im2col into a library buffer and
- * multiplied as the GEMM (oc x c kh kw) (c kh kw x oh ow) on the mp path
- * (precision mode and tuning apply).  Device pointers; returns the status. */
+ * padding; per image the GEMM (oc x c kh kw) (c kh kw x oh ow).  In FP32
+ * precision it runs as an implicit GEMM on the CUDA cores (the tile loader
+ * reads the im2col columns straight from x; no column buffer), with the mp
+ * path's rounding order (GEMM_K blocks); in the split-BF16 modes each image
+ * is expanded by im2col into a library buffer and multiplied on the mp path.
+ * Device pointers; returns the status. */
 LIBSHALOM_API int LibShalom_sconv2d_nchw(const float *x, long n, long c, long h, long w,
                                          const float *weights, long oc, long kh, long kw,
                                          long sh, long sw, long ph, long pw, float *y);

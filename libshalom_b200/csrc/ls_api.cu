@@ -843,7 +843,14 @@ int LibShalom_sconv2d_nchw(const float *x, long n, long c, long h, long w, const
     rc = LIBSHALOM_ERR_INVALID_VALUE;
   const long oh = (h + 2 * ph - kh) / sh + 1, ow = (w + 2 * pw - kw) / sw + 1;
   if (!rc && (h + 2 * ph < kh || w + 2 * pw < kw)) rc = LIBSHALOM_ERR_INVALID_VALUE;
-  if (!rc && n > 0 && !(rc = ensure_device())) {
+  // the implicit GEMM indexes k = (ci, r, q) and p = (oy, ox) in int32
+  const bool small_idx = c * kh * kw < INT32_MAX && oh * ow < INT32_MAX && c * h * w < INT32_MAX;
+  if (!rc && n > 0 && state().precision == LIBSHALOM_PREC_FP32 && small_idx &&
+      !(rc = ensure_device())) {
+    // FP32: implicit GEMM, the tile loader gathers the im2col columns (no buffer)
+    rc = conv_implicit(x, n, c, h, w, wt, oc, kh, kw, sh, sw, ph, pw, oh, ow, y);
+    if (!rc) rc = finish_launch("sconv2d_nchw");
+  } else if (!rc && n > 0 && !(rc = ensure_device())) {
     const long K = c * kh * kw, P = oh * ow;
     void *buf = nullptr;
     rc = frontend_buffer(sizeof(float) * (size_t)K * P, &buf);

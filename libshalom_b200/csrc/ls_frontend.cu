@@ -1,12 +1,14 @@
 // ls_frontend.cu -- front ends that feed the GEMM paths: the DBCSR-style
-// stack of (M, N, K, offsets into pools) -> grouped DGEMM entries, and the
-// im2col expansion of a 2-D convolution (NCHW).
+// stack of (M, N, K, offsets into pools) -> grouped DGEMM entries, the
+// im2col expansion of a 2-D convolution (NCHW), and the implicit-GEMM
+// convolution whose tile loader gathers the im2col columns itself.
 #include <cuda_runtime.h>
 
 #include <algorithm>
 
 #include "ls_common.cuh"
 #include "ls_frontend.h"
+#include "ls_simt.cuh"
 
 namespace ls {
 
@@ -47,7 +49,68 @@ __global__ void k_im2col(const float *x, long c, long h, long w, long kh, long k
   }
 }
 
+// op(B)[k][p] of the convolution GEMM y[oc][p] = wt[oc][k] col[k][p]: the
+// im2col element for k = (ci, r, q), p = (oy, ox), read from the image
+struct ConvB {
+  const float *x;  // this image, [c][h][w]
+  int h, w, kw, khw, sh, sw, ph, pw, ow;
+  __device__ __forceinline__ float operator()(const GemmArgs<float> &, long k, long p) const {
+    const int kk = (int)k, pp = (int)p;
+    const int ci = kk / khw, rq = kk - ci * khw, r = rq / kw, q = rq - r * kw;
+    const int oy = pp / ow, ox = pp - oy * ow;
+    const int iy = oy * sh - ph + r, ix = ox * sw - pw + q;
+    return (iy >= 0 && iy < h && ix >= 0 && ix < w) ? x[((long)ci * h + iy) * w + ix] : 0.0f;
+  }
+};
+
+// persistent over (image, tile_m, tile_n); per output element the mp path's
+// rounding order: FMA chains over k restarted every GEMM_K = 320 values of k,
+// the block sums added in increasing k
+template <class Cfg>
+__global__ void __launch_bounds__(Cfg::NTH)
+    k_conv_implicit(GemmArgs<float> g, ConvB b, long n_img, long img_stride, int tiles_m,
+                    int tiles_n) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  float *smem = reinterpret_cast<float *>(smem_raw);
+  const long per_img = (long)tiles_m * tiles_n;
+  for (long wi = blockIdx.x; wi < per_img * n_img; wi += gridDim.x) {
+    const long img = wi / per_img;
+    const int t = (int)(wi - img * per_img);
+    ConvB bi = b;
+    bi.x = b.x + img * img_stride;
+    simt_tile<float, Cfg, GEMM_K, ConvB>(g, (long)(t / tiles_n) * Cfg::BM,
+                                    (long)(t % tiles_n) * Cfg::BN, 0, g.K,
+                                    g.C + img * g.M * g.N, g.N, 1.0f, 0.0f, smem, bi);
+  }
+}
+
+using ConvCfg = SimtCfg<float, 64, 64, 16, 4, 4>;
+
 }  // namespace
+
+int conv_implicit(const float *x, long n, long c, long h, long w, const float *wt, long oc,
+                  long kh, long kw, long sh, long sw, long ph, long pw, long oh, long ow,
+                  float *y) {
+  State &st = state();
+  GemmArgs<float> g;
+  g.A = wt; g.B = nullptr; g.C = y;
+  g.M = oc; g.N = oh * ow; g.K = c * kh * kw;
+  g.lda = g.K; g.ldb = g.N; g.ldc = g.N;
+  g.transa = 0; g.transb = 0;
+  g.alpha = 1.0f; g.beta = 0.0f;
+  ConvB b;
+  b.x = x;
+  b.h = (int)h; b.w = (int)w; b.kw = (int)kw; b.khw = (int)(kh * kw);
+  b.sh = (int)sh; b.sw = (int)sw; b.ph = (int)ph; b.pw = (int)pw; b.ow = (int)ow;
+  const int tiles_m = (int)cdiv(g.M, ConvCfg::BM), tiles_n = (int)cdiv(g.N, ConvCfg::BN);
+  const size_t smem = sizeof(float) * ConvCfg::SMEM_ELEMS;
+  const int per_sm = occupancy_of((const void *)k_conv_implicit<ConvCfg>, ConvCfg::NTH, smem, 1);
+  const int grid = grid_for((long)tiles_m * tiles_n * n, per_sm);
+  k_conv_implicit<ConvCfg><<<grid, ConvCfg::NTH, smem, st.stream>>>(g, b, n, c * h * w, tiles_m,
+                                                                    tiles_n);
+  LS_CUDA_TRY(cudaGetLastError());
+  return LIBSHALOM_SUCCESS;
+}
 
 int stack_to_entries(const StackArgs &s, long count, LibShalom_dgemm_entry *out) {
   State &st = state();

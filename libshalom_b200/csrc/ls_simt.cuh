@@ -82,14 +82,25 @@ __device__ __forceinline__ void lds_vec<double, 4>(const double *p, double *out)
 __device__ __forceinline__ float fma_t(float a, float b, float c) { return __fmaf_rn(a, b, c); }
 __device__ __forceinline__ double fma_t(double a, double b, double c) { return __fma_rn(a, b, c); }
 
+// Where the tile reads op(B)[k][n] from: the dense row-major B of the
+// GemmArgs (the GEMM calls), or a gather such as the implicit im2col columns
+// of a convolution (ls_frontend.cu).  Only called for k < K and n < N.
+struct DenseB {
+  template <typename T>
+  __device__ __forceinline__ T operator()(const GemmArgs<T> &g, long k, long n) const {
+    return g.transb ? g.B[n * g.ldb + k] : g.B[k * g.ldb + n];
+  }
+};
+
 // Computes the tile at (m0, n0) over k in [kb, ke) and writes
 //   out[r*ldo + c] = alpha * acc + beta * out[r*ldo + c]   (beta != 0)
 //   out[r*ldo + c] = alpha * acc                           (beta == 0)
 // for the in-range part.  `smem` holds Cfg::SMEM_ELEMS elements.
-template <typename T, class Cfg, int KBLOCK>
+template <typename T, class Cfg, int KBLOCK, class BSrc = DenseB>
 __device__ __forceinline__ void simt_tile(const GemmArgs<T> &g, long m0,
                                           long n0, long kb, long ke, T *out,
-                                          long ldo, T alpha, T beta, T *smem) {
+                                          long ldo, T alpha, T beta, T *smem,
+                                          const BSrc &bsrc = BSrc()) {
   constexpr int BM = Cfg::BM, BN = Cfg::BN, BK = Cfg::BK;
   constexpr int TM = Cfg::TM, TN = Cfg::TN, NTH = Cfg::NTH;
   constexpr int PA = Cfg::PA, PB = Cfg::PB;
@@ -101,8 +112,8 @@ __device__ __forceinline__ void simt_tile(const GemmArgs<T> &g, long m0,
 
   T ra[Cfg::A_PER], rb[Cfg::B_PER];
 
-  const T *A = g.A, *B = g.B;
-  const long M = g.M, N = g.N, lda = g.lda, ldb = g.ldb;
+  const T *A = g.A;
+  const long M = g.M, N = g.N, lda = g.lda;
   const int ta = g.transa, tb = g.transb;
 
   auto load_slab = [&](long k0) {
@@ -123,7 +134,7 @@ __device__ __forceinline__ void simt_tile(const GemmArgs<T> &g, long m0,
       if (!tb) { n = e % BN; k = e / BN; } else { k = e % BK; n = e / BK; }
       long gn = n0 + n, gk = k0 + k;
       T v = T(0);
-      if (gn < N && gk < ke) v = tb ? B[gn * ldb + gk] : B[gk * ldb + gn];
+      if (gn < N && gk < ke) v = bsrc(g, gk, gn);
       rb[i] = v;
     }
   };

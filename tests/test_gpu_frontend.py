@@ -1,5 +1,6 @@
 """GPU parity of the front ends: plain calls with explicit leading dimensions
-and alpha / beta, the DBCSR-style DGEMM stack, and the im2col convolution.
+and alpha / beta, the DBCSR-style DGEMM stack, and the convolution (implicit
+GEMM in FP32, im2col + mp GEMM in the split-BF16 modes).
 
 Tolerances (normwise max|C - C_ref| / max|C_ref|): FP32 plain and split-BF16
 x6 <= 1e-6, FP64 <= 1e-14, against the FP64 / long-double oracle (torch FP64
@@ -123,6 +124,28 @@ def test_dgemm_stack(method, uniform, reset):
         M, N = Ms[i], Ns[i]
         o = co[i]
         assert normwise_err(got[o:o + M * N], ref[o:o + M * N]) <= 1e-14, r
+
+
+@pytest.mark.parametrize("n,c,h,w,oc,kh,kw,sh,sw,ph,pw", [
+    (3, 5, 11, 23, 7, 3, 5, 2, 1, 0, 2),     # rectangular kernel, mixed stride / padding
+    (2, 64, 30, 30, 96, 3, 3, 1, 1, 1, 1),   # K = 576: 36 K-slabs, 2 x 15 output tiles
+    (1, 1, 9, 9, 1, 9, 9, 1, 1, 4, 4),       # one channel, kernel as large as the image
+    (4, 8, 13, 13, 130, 1, 1, 3, 3, 0, 0),   # 1 x 1, stride 3, oc past one 64-row tile
+    (2, 256, 14, 14, 64, 3, 3, 1, 1, 1, 1),  # K = 2304: the GEMM_K = 320 blocked chains
+])
+def test_sconv2d_implicit_fp32(n, c, h, w, oc, kh, kw, sh, sw, ph, pw, reset):
+    """FP32 convolution as an implicit GEMM (the tile loader gathers the im2col
+    columns from the image; no column buffer), against torch FP64 conv2d."""
+    import torch
+    rng = np.random.default_rng(n + c + h + w + oc)
+    x = rng.uniform(-1, 1, size=(n, c, h, w)).astype(np.float32)
+    wt = rng.uniform(-1, 1, size=(oc, c, kh, kw)).astype(np.float32)
+    ref = torch.nn.functional.conv2d(torch.from_numpy(x).double(), torch.from_numpy(wt).double(),
+                                     stride=(sh, sw), padding=(ph, pw)).numpy()
+    y = torch.full(ref.shape, float("nan"), device="cuda", dtype=torch.float32)
+    ls.set_precision(ls.PREC_FP32)
+    ls.sconv2d_nchw(to_dev(x), n, c, h, w, to_dev(wt), oc, kh, kw, sh, sw, ph, pw, y)
+    assert normwise_err(to_host(y), ref) <= 1e-6
 
 
 @pytest.mark.parametrize("prec", [ls.PREC_FP32, ls.PREC_BF16X6])
