@@ -558,19 +558,22 @@ done:
 // Warp-specialized TMA variant (operands that TMA can address: 16-byte
 // aligned bases and row strides).  Roles, all connected by mbarriers:
 //   warp 0      producer: one thread issues cp.async.bulk.tensor loads of the
-//               A and op(B) slabs into a 4-deep FP32 ring (A and B (Trans)
+//               A and op(B) slabs into a 3-deep FP32 ring (A and B (Trans)
 //               boxes land 128-byte swizzled)
 //   warp 1      MMA: one thread issues tcgen05.mma into one of two TMEM
 //               accumulator sets (512 columns), so the epilogue of one tile or
 //               accumulation chunk overlaps the MMAs of the next
-//   warps 2-9   converters: FP32 slab -> split BF16 core matrices (2 buffers)
-//   warps 10-17 epilogue: TMEM -> registers -> C (and the register fold of the
-//               long-K chunks).  With beta = 0 and a TMA-addressable C (one
-//               GEMM per tile) each warp stages 32 rows x 32 columns of C in
-//               its own 4 KB shared buffer (128-byte swizzle) and writes them
+//   converters  FP32 slab -> split BF16 core matrices (2 buffers): 8 or 16
+//               warps (WsRoles below)
+//   epilogue    TMEM -> registers -> C (and the register fold of the long-K
+//               chunks): 8 or 4 warps.  With beta = 0 and a TMA-addressable C
+//               (one GEMM per tile) each warp stages 32 rows x 32 columns of C
+//               in a 4 KB shared buffer (128-byte swizzle) and writes them
 //               with one cp.async.bulk.tensor store: full-line writes instead
-//               of one 16-byte piece per row and thread, which would occupy the
-//               L1 data path the MMAs and converters share.
+//               of one 16-byte piece per row and thread, which would occupy
+//               the L1 data path the MMAs and converters share.
+// The shared-memory data path bounds the kernel: one MMA of 128 x 128 x 16
+// reads 8 KB of operands in its 64 cycles, the SM's whole 128 B/clk.
 // ===========================================================================
 constexpr int WS_STAGES = 3;
 constexpr int WS_STAGE_BYTES = 32768;                           // A 16 KB + B 16 KB
