@@ -101,6 +101,37 @@ def test_tc_batch_every_gemm_and_nothing_past_c(M, N, K, transb, mode_setter):
         _check(C[g], A[g], B[g], transb, ls.PREC_BF16X6)
 
 
+@pytest.mark.parametrize("mode", [ls.PREC_BF16X6, ls.PREC_BF16X3])
+@pytest.mark.parametrize("transb", [0, 1])
+@pytest.mark.parametrize("M,N,K", [(100, 1, 40), (130, 16, 33), (96, 17, 300), (200, 32, 64),
+                                   (70, 29, 700)])
+def test_tc_narrow_tiles(M, N, K, transb, mode, mode_setter, staging):
+    """Tiles of at most 32 columns, one GEMM per tile (MMA N of 16 or 32),
+    short K and the long-K register fold."""
+    count = 5
+    A, B, _, C = _strided(mode, transb, M, N, K, count, seed=M + 3 * N + K + transb)
+    for g in range(count):
+        _check(C[g], A[g], B[g], transb, mode)
+
+
+@pytest.mark.parametrize("mode", [ls.PREC_BF16X6, ls.PREC_BF16X3])
+@pytest.mark.parametrize("splits", [0, 1, 5])
+def test_tc_narrow_mp_long_k(splits, mode, mode_setter):
+    """A tall, 32-column GEMM with long K (the 20480 x 32 x 20480 shape family)
+    through sgemm_mp, with and without split-K."""
+    import torch
+    M, N, K = 1536, 32, 4160
+    A, B = orc.gemm_inputs_f32(M + N + K + splits, M, N, K, 0)
+    dC = torch.full((M, N), float("nan"), device="cuda")
+    ls.set_precision(mode)
+    ls.set_splitk(splits)
+    try:
+        ls.sgemm_mp(0, 0, dC, to_dev(A), to_dev(B), M, N, K)
+    finally:
+        ls.set_splitk(0)
+    _check(to_host(dC), A, B, 0, mode)
+
+
 def test_tc_alpha_beta(mode_setter):
     A, B, C0, C = _strided(ls.PREC_BF16X6, 1, 24, 40, 56, 20, seed=5, alpha=-0.5, beta=1.0)
     for g in range(20):
