@@ -123,3 +123,45 @@ def test_no_device_reported_without_gpu():
     fake = 0x1000
     st = ls.sgemm(0, 0, fake, fake, fake, 4, 4, 4, check=False)
     assert st == ls.ERR_NO_DEVICE
+
+
+def test_host_calls_validate_before_device_work():
+    import numpy as np
+    a = np.zeros(64, np.float32)
+    assert ls.sgemm_host(2, 0, a, a, a, 4, 4, 4, check=False) == ls.ERR_INVALID_VALUE
+    assert ls.dgemm_host(0, 0, None, None, None, -1, 4, 4, check=False) == ls.ERR_INVALID_VALUE
+    assert ls.sgemm_mp_host(0, 0, None, None, None, 4, 4, 4, check=False) == ls.ERR_INVALID_VALUE
+    # M == 0: nothing to copy or compute
+    assert ls.sgemm_host(0, 0, None, None, None, 0, 4, 4, check=False) == ls.SUCCESS
+    # overlapping outputs of a batch cannot be copied back
+    st = ls.sgemm_batched_strided_host(0, 4, 4, 4, 1.0, a, 16, a, 16, 0.0, a, 8, 2, check=False)
+    assert st == ls.ERR_INVALID_VALUE
+
+
+def test_host_pointer_of_arrays_and_cpu_tensors():
+    import numpy as np
+    a = np.zeros(8, np.float32)
+    assert ls._hptr(a) == a.ctypes.data
+    assert ls._hptr(None) is None and ls._hptr(1234) == 1234
+    torch = pytest.importorskip("torch")
+    t = torch.zeros(8)
+    assert ls._hptr(t) == t.data_ptr()
+
+    class DeviceTensor:  # stands in for a CUDA tensor on a machine without one
+        is_cuda = True
+
+        def data_ptr(self):
+            return 0x1000
+    with pytest.raises(ValueError):
+        ls._hptr(DeviceTensor())
+
+
+def test_convolution_arguments_validated():
+    fake = 0x1000
+    # kernel taller than the padded image, negative padding, zero stride
+    assert ls.sconv2d_nchw(fake, 1, 1, 4, 4, fake, 1, 7, 3, 1, 1, 1, 1, fake,
+                           check=False) == ls.ERR_INVALID_VALUE
+    assert ls.sconv2d_nchw(fake, 1, 1, 4, 4, fake, 1, 3, 3, 1, 1, -1, 0, fake,
+                           check=False) == ls.ERR_INVALID_VALUE
+    assert ls.sconv2d_nchw(fake, 1, 1, 4, 4, fake, 1, 3, 3, 0, 1, 1, 1, fake,
+                           check=False) == ls.ERR_INVALID_VALUE
