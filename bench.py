@@ -524,6 +524,30 @@ def wl_single(args):
     ms_async_graph = _time_events(torch, s, lambda: ls.sgemm(0, 1, C, A, B, 80, 80, 80),
                                   args.steps, args.warmup)
     ls.set_graph_cache(False)
+    # many independent calls: recorded in the host-pinned ring, one flush
+    # (wall clock from the first call to the flush's completion)
+    n_calls = 1000
+    outs = [torch.empty((80, 80), device="cuda") for _ in range(n_calls)]
+
+    def deferred():
+        ls.defer_begin()
+        for Ci in outs:
+            ls.sgemm(0, 1, Ci, A, B, 80, 80, 80)
+        ls.defer_flush()
+        s.synchronize()
+
+    def direct():
+        for Ci in outs:
+            ls.sgemm(0, 1, Ci, A, B, 80, 80, 80)
+        s.synchronize()
+    per_call = {}
+    for name, fn in (("deferred", deferred), ("direct", direct)):
+        for _ in range(max(args.warmup, 3)):
+            fn()
+        t0 = time.perf_counter()
+        for _ in range(3):
+            fn()
+        per_call[name] = (time.perf_counter() - t0) / (3 * n_calls) * 1e6
     _emit("single SGEMM NT 80^3 GFLOP/s (synchronous calls, as the reference API)",
           flops / (ms_sync / 1e3) / 1e9, "GFLOP/s", ms_sync, args,
           {"workload": "LibShalom_sgemm(NoTrans, Trans) M=N=K=80, C overwritten, one call per step"},
@@ -531,7 +555,10 @@ def wl_single(args):
           {"dtype": "f32", "latency_us_sync": ms_sync * 1e3, "latency_us_stream": ms_async * 1e3,
            "latency_us_sync_graph_cache": ms_sync_graph * 1e3,
            "latency_us_stream_graph_cache": ms_async_graph * 1e3,
-           "gflops_stream_ordered": flops / (ms_async / 1e3) / 1e9, "gpu_launches": args.steps})
+           "gflops_stream_ordered": flops / (ms_async / 1e3) / 1e9,
+           "us_per_call_1000_calls_stream": per_call["direct"],
+           "us_per_call_1000_calls_deferred": per_call["deferred"],
+           "gpu_launches": args.steps})
 
 
 IRREGULAR = [(64, 3136, 576), (128, 784, 1152), (256, 196, 2304), (512, 49, 4608),

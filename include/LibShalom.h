@@ -221,6 +221,29 @@ LIBSHALOM_API int LibShalom_sgemm_batched_strided_host(int transb, long M, long 
                                                        long strideB, float beta, float *C,
                                                        long strideC, long count);
 
+/* Deferred drop-in calls (no counterpart in the reference): after
+ * LibShalom_defer_begin, LibShalom_sgemm, LibShalom_sgemm_mp and
+ * LibShalom_dgemm (device pointers, transa == NoTrans) are recorded as
+ * entries in a page-locked host ring instead of launched, and return at once;
+ * LibShalom_defer_flush copies the recorded entries to the device in one
+ * transfer per precision, runs them as grouped batches (the
+ * LibShalom_sgemm_batched / _dgemm_batched kernels under the current
+ * precision and DGEMM method) and ends the deferral.  Many small calls then
+ * cost a few launches instead of one each.  Plain FP32 and FP64 FMA results
+ * are the same as the direct LibShalom_sgemm / LibShalom_dgemm calls';
+ * LibShalom_sgemm_mp's GEMM_K blocking is not applied.  Order: a call that
+ * reads a matrix a pending call writes, writes one a pending call reads, or
+ * writes a pending call's C other than the directly preceding call's (same M
+ * and N) first flushes the pending calls, and calls that cannot be recorded
+ * (transa == Trans, sizes past 2^31) flush and then run directly; matrices
+ * that overlap without sharing a base pointer are the caller's to keep
+ * apart.  Results are ready once the flush has completed (synchronous mode)
+ * or in stream order after it.  LibShalom_defer_pending returns the number
+ * of recorded calls not yet launched. */
+LIBSHALOM_API int LibShalom_defer_begin(void);
+LIBSHALOM_API int LibShalom_defer_flush(void);
+LIBSHALOM_API int LibShalom_defer_pending(void);
+
 /* Split-K SGEMM that allocates nothing.  No counterpart in the reference.
  * For callers that cannot allocate device memory (their GPU memory is owned
  * by another allocator, or a cudaMalloc in the middle of a call is not

@@ -57,6 +57,7 @@ EXPORTED = (
     "LibShalom_dgemm_batched", "LibShalom_sgemm_mp_noalloc",
     "LibShalom_sgemm_host", "LibShalom_sgemm_mp_host", "LibShalom_dgemm_host",
     "LibShalom_sgemm_batched_strided_host",
+    "LibShalom_defer_begin", "LibShalom_defer_flush", "LibShalom_defer_pending",
 )
 
 _L = ctypes.c_long
@@ -125,6 +126,9 @@ _SIGS = {
     "LibShalom_dgemm_host": (None, [_I, _I, _P, _P, _P, _L, _L, _L]),
     "LibShalom_sgemm_batched_strided_host": (_I, [_I, _L, _L, _L, _F, _P, _L, _P, _L, _F, _P,
                                                   _L, _L]),
+    "LibShalom_defer_begin": (_I, []),
+    "LibShalom_defer_flush": (_I, []),
+    "LibShalom_defer_pending": (_I, []),
 }
 
 _lib = None
@@ -235,6 +239,23 @@ def dgemm_host(transa, transb, C, A, B, M, N, K, check=True) -> int:
     if check:
         _check(st, "LibShalom_dgemm_host")
     return st
+
+
+def defer_begin() -> None:
+    """Record the following sgemm / sgemm_mp / dgemm calls in the host ring."""
+    _check(lib().LibShalom_defer_begin(), "LibShalom_defer_begin")
+
+
+def defer_flush(check=True) -> int:
+    """Launch the recorded calls as grouped batches and end the deferral."""
+    st = lib().LibShalom_defer_flush()
+    if check:
+        _check(st, "LibShalom_defer_flush")
+    return st
+
+
+def defer_pending() -> int:
+    return lib().LibShalom_defer_pending()
 
 
 def set_thread_nums(num: int) -> None:

@@ -7,6 +7,7 @@
 
 #include <algorithm>
 #include <unordered_map>
+#include <unordered_set>
 
 #include "ls_common.cuh"
 #include "ls_frontend.h"
@@ -480,6 +481,181 @@ static int gemm_host(int transa, int transb, T *C, const T *A, const T *B, long 
 
 }  // namespace ls
 
+// ---------------------------------------------------------------------------
+// Deferred drop-in calls: a host-pinned descriptor ring.  Between
+// LibShalom_defer_begin and LibShalom_defer_flush the drop-in calls record an
+// entry (pointers, sizes) in page-locked host memory instead of launching; the
+// flush copies the FP32 and the FP64 entries to the device in one transfer
+// each and runs them as grouped batches, so N small calls cost two or three
+// launches instead of N.  Recorded calls keep their sequential meaning for
+// exact-pointer aliasing: a call that reads a matrix an earlier pending call
+// writes, writes a matrix an earlier pending call reads, or writes a C an
+// earlier pending call wrote (other than the directly preceding call with
+// the same M and N, which the grouped kernels apply in order) first flushes
+// the pending calls.  Calls whose matrices overlap without sharing a base
+// pointer are the caller's to keep apart.
+// ---------------------------------------------------------------------------
+namespace ls {
+
+struct DeferSets {
+  std::unordered_set<const void *> reads, writes;
+  const void *last_c = nullptr;
+  long last_m = -1, last_n = -1;
+  void clear() {
+    reads.clear();
+    writes.clear();
+    last_c = nullptr;
+    last_m = last_n = -1;
+  }
+};
+static DeferSets &defer_sets() {
+  static DeferSets d;
+  return d;
+}
+
+// no flush's copy still reads the rings
+static int ring_idle() {
+  State &st = state();
+  if (st.ring_busy) {
+    LS_CUDA_TRY(cudaEventSynchronize(st.ring_ev));
+    st.ring_busy = false;
+  }
+  return LIBSHALOM_SUCCESS;
+}
+
+template <typename E>
+static int ring_grow(E **ring, long *cap, long need) {
+  if (need <= *cap) return LIBSHALOM_SUCCESS;
+  long ncap = std::max(need, std::max(256L, 2 * *cap));
+  E *n = nullptr;
+  if (cudaHostAlloc(reinterpret_cast<void **>(&n), sizeof(E) * (size_t)ncap,
+                    cudaHostAllocDefault) != cudaSuccess) {
+    cudaGetLastError();
+    return LIBSHALOM_ERR_ALLOC;
+  }
+  if (*ring) {
+    memcpy(n, *ring, sizeof(E) * (size_t)*cap);
+    cudaFreeHost(*ring);
+  }
+  *ring = n;
+  *cap = ncap;
+  return LIBSHALOM_SUCCESS;
+}
+
+// launches the pending entries (stream-ordered) and empties the rings
+static int defer_launch() {
+  State &st = state();
+  DeferSets &ds = defer_sets();
+  const long ns = st.ring_s_n, nd = st.ring_d_n;
+  ds.clear();
+  if (ns == 0 && nd == 0) return LIBSHALOM_SUCCESS;
+  st.ring_s_n = st.ring_d_n = 0;
+  int rc = ensure_device();
+  if (rc) return rc;
+  if (!st.ring_ev) LS_CUDA_TRY(cudaEventCreateWithFlags(&st.ring_ev, cudaEventDisableTiming));
+  const size_t bs = sizeof(LibShalom_sgemm_entry) * (size_t)ns;
+  const size_t bd = sizeof(LibShalom_dgemm_entry) * (size_t)nd;
+  void *buf = nullptr;
+  if ((rc = frontend_buffer((bs + 255) / 256 * 256 + bd, &buf))) return rc;
+  auto *dev_s = static_cast<LibShalom_sgemm_entry *>(buf);
+  auto *dev_d = reinterpret_cast<LibShalom_dgemm_entry *>(static_cast<unsigned char *>(buf) +
+                                                          (bs + 255) / 256 * 256);
+  if (ns) LS_CUDA_TRY(cudaMemcpyAsync(dev_s, st.ring_s, bs, cudaMemcpyHostToDevice, st.stream));
+  if (nd) LS_CUDA_TRY(cudaMemcpyAsync(dev_d, st.ring_d, bd, cudaMemcpyHostToDevice, st.stream));
+  LS_CUDA_TRY(cudaEventRecord(st.ring_ev, st.stream));
+  st.ring_busy = true;
+  if (ns)
+    rc = st.precision == LIBSHALOM_PREC_FP32 ? run_grouped_s(dev_s, ns)
+                                             : tc_sgemm_grouped(dev_s, ns, st.precision);
+  if (!rc && nd)
+    rc = st.dgemm_method == LIBSHALOM_DGEMM_FMA
+             ? run_grouped_d(dev_d, nd)
+             : run_dgemm_warp(dev_d, nd, st.dgemm_method, st.ozaki_slices);
+  if (rc) return rc;
+  return finish_launch("defer_flush");
+}
+
+// Records a drop-in call while deferring.  Returns 1 when the call was
+// recorded (or is an empty problem), 0 when it must run directly (transa, or
+// sizes past the entries' int32 fields), or a negative status on failure.
+template <typename T>
+static int defer_record(int transa, int transb, T *C, const T *A, const T *B, long M, long N,
+                        long K, int *status) {
+  State &st = state();
+  *status = LIBSHALOM_SUCCESS;
+  if ((transa != NoTrans && transa != Trans) || (transb != NoTrans && transb != Trans) ||
+      M < 0 || N < 0 || K < 0) {
+    *status = LIBSHALOM_ERR_INVALID_VALUE;
+    return 1;
+  }
+  if (M == 0 || N == 0) return 1;
+  if (!C || (K > 0 && (!A || !B))) {
+    *status = LIBSHALOM_ERR_INVALID_VALUE;
+    return 1;
+  }
+  DeferSets &ds = defer_sets();
+  const bool fits = transa == NoTrans && M <= INT32_MAX && N <= INT32_MAX && K <= INT32_MAX;
+  const bool waw_ok = C == ds.last_c && M == ds.last_m && N == ds.last_n;
+  const bool hazard = ds.writes.count(A) || ds.writes.count(B) || ds.reads.count(C) ||
+                      (ds.writes.count(C) && !waw_ok);
+  if (!fits || hazard) {
+    // run (or start a new batch) after everything recorded so far
+    const int rc = defer_launch();
+    if (rc) {
+      *status = rc;
+      return 1;
+    }
+    if (!fits) return 0;
+  }
+  int rc = ring_idle();
+  if (!rc) {
+    if (sizeof(T) == 4) rc = ring_grow(&st.ring_s, &st.ring_s_cap, st.ring_s_n + 1);
+    else rc = ring_grow(&st.ring_d, &st.ring_d_cap, st.ring_d_n + 1);
+  }
+  if (rc) {
+    *status = rc;
+    return 1;
+  }
+  const int32_t ldb = (int32_t)(transb ? K : N);
+  if (sizeof(T) == 4) {
+    LibShalom_sgemm_entry &e = st.ring_s[st.ring_s_n++];
+    e.A = reinterpret_cast<const float *>(A);
+    e.B = reinterpret_cast<const float *>(B);
+    e.C = reinterpret_cast<float *>(C);
+    e.M = (int32_t)M; e.N = (int32_t)N; e.K = (int32_t)K; e.transb = transb;
+    e.lda = (int32_t)K; e.ldb = ldb; e.ldc = (int32_t)N;
+    e.alpha = 1.0f; e.beta = 0.0f; e.reserved = 0;
+  } else {
+    LibShalom_dgemm_entry &e = st.ring_d[st.ring_d_n++];
+    e.A = reinterpret_cast<const double *>(A);
+    e.B = reinterpret_cast<const double *>(B);
+    e.C = reinterpret_cast<double *>(C);
+    e.M = (int32_t)M; e.N = (int32_t)N; e.K = (int32_t)K; e.transb = transb;
+    e.lda = (int32_t)K; e.ldb = ldb; e.ldc = (int32_t)N;
+    e.alpha = 1.0; e.beta = 0.0; e.reserved = 0;
+  }
+  ds.reads.insert(A);
+  ds.reads.insert(B);
+  ds.writes.insert(C);
+  ds.last_c = C;
+  ds.last_m = M;
+  ds.last_n = N;
+  return 1;
+}
+
+// the drop-in calls: recorded while deferring, else run now
+template <typename T>
+static int dropin(int kind, int transa, int transb, T *C, const T *A, const T *B, long M,
+                  long N, long K, bool mp) {
+  if (state().deferring) {
+    int status = LIBSHALOM_SUCCESS;
+    if (defer_record<T>(transa, transb, C, A, B, M, N, K, &status) != 0) return status;
+  }
+  return gemm_cached<T>(kind, transa, transb, C, A, B, M, N, K, mp);
+}
+
+}  // namespace ls
+
 using namespace ls;
 
 extern "C" {
@@ -487,19 +663,40 @@ extern "C" {
 void LibShalom_sgemm(int transa, int transb, float *C, float *A, float *B, long M, long N,
                      long K) {
   std::lock_guard<std::mutex> lk(state().mu);
-  set_error(gemm_cached<float>(0, transa, transb, C, A, B, M, N, K, false));
+  set_error(dropin<float>(0, transa, transb, C, A, B, M, N, K, false));
 }
 
 void LibShalom_sgemm_mp(int transa, int transb, float *C, float *A, float *B, long M, long N,
                         long K) {
   std::lock_guard<std::mutex> lk(state().mu);
-  set_error(gemm_cached<float>(1, transa, transb, C, A, B, M, N, K, true));
+  set_error(dropin<float>(1, transa, transb, C, A, B, M, N, K, true));
 }
 
 void LibShalom_dgemm(int transa, int transb, double *C, double *A, double *B, long M, long N,
                      long K) {
   std::lock_guard<std::mutex> lk(state().mu);
-  set_error(gemm_cached<double>(2, transa, transb, C, A, B, M, N, K, false));
+  set_error(dropin<double>(2, transa, transb, C, A, B, M, N, K, false));
+}
+
+int LibShalom_defer_begin(void) {
+  std::lock_guard<std::mutex> lk(state().mu);
+  state().deferring = 1;
+  set_error(LIBSHALOM_SUCCESS);
+  return LIBSHALOM_SUCCESS;
+}
+
+int LibShalom_defer_flush(void) {
+  std::lock_guard<std::mutex> lk(state().mu);
+  const int rc = defer_launch();
+  state().deferring = 0;
+  set_error(rc);
+  return rc;
+}
+
+int LibShalom_defer_pending(void) {
+  std::lock_guard<std::mutex> lk(state().mu);
+  const long n = state().ring_s_n + state().ring_d_n;
+  return (int)std::min(n, (long)INT32_MAX);
 }
 
 void LibShalom_set_thread_nums(int num) {
@@ -643,6 +840,17 @@ void LibShalom_finalize(void) {
   State &st = state();
   if (st.ws || st.fe) cudaStreamSynchronize(st.stream);
   graph_cache_clear();
+  if (st.ring_busy && st.ring_ev) cudaEventSynchronize(st.ring_ev);
+  if (st.ring_ev) cudaEventDestroy(st.ring_ev);
+  if (st.ring_s) cudaFreeHost(st.ring_s);
+  if (st.ring_d) cudaFreeHost(st.ring_d);
+  st.ring_ev = nullptr;
+  st.ring_s = nullptr;
+  st.ring_d = nullptr;
+  st.ring_s_n = st.ring_s_cap = st.ring_d_n = st.ring_d_cap = 0;
+  st.ring_busy = false;
+  st.deferring = 0;
+  defer_sets().clear();
   if (st.hs_device >= 0) {
     int cur = -1;
     cudaGetDevice(&cur);

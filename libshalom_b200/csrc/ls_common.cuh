@@ -72,6 +72,15 @@ struct State {
   cudaStream_t hs_in = nullptr, hs_out = nullptr;
   cudaEvent_t hs_ev_in[3] = {}, hs_ev_done[3] = {}, hs_ev_out[3] = {};
   unsigned hs_next = 0;
+  // deferred drop-in calls (LibShalom_defer_begin .. LibShalom_defer_flush):
+  // entries in page-locked host rings, copied to the device in one transfer
+  // per precision at the flush; ring_ev marks that transfer's completion
+  int deferring = 0;
+  LibShalom_sgemm_entry *ring_s = nullptr;
+  LibShalom_dgemm_entry *ring_d = nullptr;
+  long ring_s_n = 0, ring_s_cap = 0, ring_d_n = 0, ring_d_cap = 0;
+  cudaEvent_t ring_ev = nullptr;
+  bool ring_busy = false;  // a flush's copies may still read the rings
 };
 
 State &state();
