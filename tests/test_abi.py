@@ -165,3 +165,15 @@ def test_convolution_arguments_validated():
                            check=False) == ls.ERR_INVALID_VALUE
     assert ls.sconv2d_nchw(fake, 1, 1, 4, 4, fake, 1, 3, 3, 0, 1, 1, 1, fake,
                            check=False) == ls.ERR_INVALID_VALUE
+
+
+def test_deferral_without_calls_and_invalid_calls():
+    # an empty deferred section launches nothing; invalid calls are rejected
+    # while deferring just as outside it
+    ls.defer_begin()
+    fake = 0x1000
+    assert ls.sgemm(2, 0, fake, fake, fake, 4, 4, 4, check=False) == ls.ERR_INVALID_VALUE
+    assert ls.dgemm(0, 0, None, None, None, 4, 4, 4, check=False) == ls.ERR_INVALID_VALUE
+    assert ls.sgemm(0, 0, None, None, None, 0, 4, 4, check=False) == ls.SUCCESS
+    assert ls.defer_pending() == 0
+    assert ls.defer_flush(check=False) == ls.SUCCESS
