@@ -235,7 +235,9 @@ LIBSHALOM_API int LibShalom_sgemm_batched_strided_host(int transb, long M, long 
  * reads a matrix a pending call writes, writes one a pending call reads, or
  * writes a pending call's C other than the directly preceding call's (same M
  * and N) first flushes the pending calls, and calls that cannot be recorded
- * (transa == Trans, sizes past 2^31) flush and then run directly; matrices
+ * (transa == Trans, or M N K above 128^3: the grouped kernels give each call
+ * to one CTA, so larger calls run faster directly) flush and then run
+ * directly; matrices
  * that overlap without sharing a base pointer are the caller's to keep
  * apart.  Results are ready once the flush has completed (synchronous mode)
  * or in stream order after it.  LibShalom_defer_pending returns the number

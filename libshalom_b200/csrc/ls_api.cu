@@ -575,9 +575,13 @@ static int defer_launch() {
   return finish_launch("defer_flush");
 }
 
+// Largest call worth recording (M N K): the grouped kernels give each call to
+// one CTA, so a larger call runs faster directly, over many CTAs.
+constexpr double DEFER_MAX_MNK = 2097152.0;  // 128^3
+
 // Records a drop-in call while deferring.  Returns 1 when the call was
-// recorded (or is an empty problem), 0 when it must run directly (transa, or
-// sizes past the entries' int32 fields), or a negative status on failure.
+// recorded (or is an empty problem, or failed), 0 when it must run directly
+// (transa, or M N K above DEFER_MAX_MNK) after the pending calls.
 template <typename T>
 static int defer_record(int transa, int transb, T *C, const T *A, const T *B, long M, long N,
                         long K, int *status) {
@@ -594,7 +598,7 @@ static int defer_record(int transa, int transb, T *C, const T *A, const T *B, lo
     return 1;
   }
   DeferSets &ds = defer_sets();
-  const bool fits = transa == NoTrans && M <= INT32_MAX && N <= INT32_MAX && K <= INT32_MAX;
+  const bool fits = transa == NoTrans && (double)M * (double)N * (double)K <= DEFER_MAX_MNK;
   const bool waw_ok = C == ds.last_c && M == ds.last_m && N == ds.last_n;
   const bool hazard = ds.writes.count(A) || ds.writes.count(B) || ds.reads.count(C) ||
                       (ds.writes.count(C) && !waw_ok);

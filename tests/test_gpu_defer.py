@@ -109,6 +109,27 @@ def test_deferred_transa_call_runs_directly_in_order(reset):
     assert np.array_equal(to_host(C2), orc.sgemm_kseq(At, B, 0, transa=1))
 
 
+def test_deferred_large_call_runs_directly(reset):
+    """A call above 128^3 (M N K) is not recorded: the pending calls are
+    launched, then it runs on the direct path."""
+    import torch
+    A, B = orc.gemm_inputs_f32(8, 16, 16, 16, 0)
+    dA, dB = to_dev(A), to_dev(B)
+    C1 = torch.empty(16, 16, device="cuda")
+    M, N, K = 300, 200, 100
+    L, R = orc.gemm_inputs_f32(9, M, N, K, 0)
+    dL, dR = to_dev(L), to_dev(R)
+    C2 = torch.empty(M, N, device="cuda")
+    ls.defer_begin()
+    ls.sgemm(0, 0, C1, dA, dB, 16, 16, 16)
+    assert ls.defer_pending() == 1
+    ls.sgemm(0, 0, C2, dL, dR, M, N, K)
+    assert ls.defer_pending() == 0
+    ls.defer_flush()
+    assert np.array_equal(to_host(C1), orc.sgemm_kseq(A, B, 0))
+    assert np.array_equal(to_host(C2), orc.sgemm_kseq(L, R, 0))
+
+
 def test_deferred_split_bf16_on_a_side_stream(reset):
     import torch
     rng = np.random.default_rng(11)
