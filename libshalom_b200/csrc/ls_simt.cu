@@ -340,8 +340,9 @@ int run_gemm_splitk_external(const GemmArgs<float> &g, int splits, float *partia
   int ncfg;
   const CfgInfo *cfgs = Dispatch<float>::cfgs(&ncfg);
   const int cfg = pick_cfg(cfgs, ncfg, g.M, g.N, g.K, st.num_sms, st.thread_cap);
-  long kchunk = cdiv(cdiv(g.K, splits), 320) * 320;  // keep GEMM_K blocks aligned
-  const int used = (int)cdiv(g.K, kchunk);
+  // K slices stay whole GEMM_K blocks; K = 0 is one empty slice (C = beta C)
+  const long kchunk = g.K > 0 ? cdiv(cdiv(g.K, splits), 320) * 320 : 1;
+  const int used = g.K > 0 ? (int)cdiv(g.K, kchunk) : 1;
   int rc = Dispatch<float>::single(cfg, g, used, kchunk, partial, 0, 0, true);
   if (rc || used == 1) return rc;  // one slice: the tile kernel wrote C itself
   const long total = g.M * g.N;
