@@ -8,7 +8,11 @@
  * callers relink against this library after recompiling.
  *
  * Differences a caller must know:
- *   - A, B and C are DEVICE pointers (cudaMalloc'd or managed memory).
+ *   - A, B and C are meant to be DEVICE pointers (cudaMalloc'd or managed
+ *     memory).  The drop-in calls also accept the reference's own use, HOST
+ *     buffers (malloc'd or page-locked; classified with
+ *     cudaPointerGetAttributes): such a call runs as the matching _host call
+ *     below, copying its operands through the library's staging slots.
  *   - Calls are synchronous by default (C is final when the call returns),
  *     as in the reference; LibShalom_set_sync(0) makes them stream-ordered
  *     on the stream given to LibShalom_set_stream().
@@ -103,7 +107,9 @@ LIBSHALOM_API int LibShalom_get_last_error(void);
 /* Static description of a status code. */
 LIBSHALOM_API const char *LibShalom_error_string(int status);
 
-/* Stream for all later launches (a cudaStream_t; NULL = default stream). */
+/* Stream for all later launches (a cudaStream_t; NULL = default stream).
+ * Switching streams first waits for the library's work on the old stream,
+ * whose calls may still read the library's device buffers. */
 LIBSHALOM_API int LibShalom_set_stream(void *stream);
 /* 1 (default): calls return after the result is written.  0: calls are
  * stream-ordered and return after the launch. */
@@ -153,6 +159,20 @@ LIBSHALOM_API int LibShalom_get_plan(int *tile_config, int *splits, int *table_e
  * strides; 0 = always the cp.async kernel (any alignment).  Results are the
  * same either way. */
 LIBSHALOM_API int LibShalom_set_tma(int enable);
+
+/* Self-check of failure detection (no counterpart in the reference).  Every
+ * wait of the library's tensor-core kernels on an mbarrier is bounded: after
+ * its limit the waiting role sets an abort flag and a device status word,
+ * the other roles give up when they see the flag, the kernel frees what it
+ * holds and returns, and a synchronous call reports
+ * LIBSHALOM_ERR_DEVICE_TIMEOUT instead of hanging the GPU.  This call runs
+ * that path on purpose: a one-CTA kernel waits on an mbarrier that nothing
+ * arrives at (one warp for `iterations` polls, 0 = 4096, the other with the
+ * kernels' own limit).  Synchronous.  Returns LIBSHALOM_ERR_DEVICE_TIMEOUT
+ * when the waits expired, the kernel returned and the host read the status
+ * (the expected outcome, after which the context stays usable);
+ * LIBSHALOM_SUCCESS would mean the expiry went unreported. */
+LIBSHALOM_API int LibShalom_selftest_wait_expiry(int iterations);
 
 /* Release the library's device workspace and cached plans. */
 LIBSHALOM_API void LibShalom_finalize(void);
@@ -227,8 +247,8 @@ LIBSHALOM_API int LibShalom_sgemm_batched_strided_host(int transb, long M, long 
  * entries in a page-locked host ring instead of launched, and return at once;
  * LibShalom_defer_flush copies the recorded entries to the device in one
  * transfer per precision, runs them as grouped batches (the
- * LibShalom_sgemm_batched / _dgemm_batched kernels under the current
- * precision and DGEMM method) and ends the deferral.  Many small calls then
+ * LibShalom_sgemm_batched / _dgemm_batched kernels under the precision and
+ * DGEMM method of the recorded calls) and ends the deferral.  Many small calls then
  * cost a few launches instead of one each.  Plain FP32 and FP64 FMA results
  * are the same as the direct LibShalom_sgemm / LibShalom_dgemm calls';
  * LibShalom_sgemm_mp's GEMM_K blocking is not applied.  Order: a call that
@@ -239,7 +259,12 @@ LIBSHALOM_API int LibShalom_sgemm_batched_strided_host(int transb, long M, long 
  * to one CTA, so larger calls run faster directly) flush and then run
  * directly; matrices
  * that overlap without sharing a base pointer are the caller's to keep
- * apart.  Results are ready once the flush has completed (synchronous mode)
+ * apart.  Every other call that launches work (the batched, _ex, _host,
+ * stack, convolution and no-allocation calls) launches the pending calls
+ * first, and so do LibShalom_set_stream, _set_precision, _set_dgemm_method,
+ * _set_thread_nums and LibShalom_finalize: pending calls run under the
+ * settings they were recorded with, on the device that was current then,
+ * and are never dropped.  Results are ready once the flush has completed (synchronous mode)
  * or in stream order after it.  LibShalom_defer_pending returns the number
  * of recorded calls not yet launched. */
 LIBSHALOM_API int LibShalom_defer_begin(void);

@@ -58,6 +58,7 @@ EXPORTED = (
     "LibShalom_sgemm_host", "LibShalom_sgemm_mp_host", "LibShalom_dgemm_host",
     "LibShalom_sgemm_batched_strided_host",
     "LibShalom_defer_begin", "LibShalom_defer_flush", "LibShalom_defer_pending",
+    "LibShalom_selftest_wait_expiry",
 )
 
 _L = ctypes.c_long
@@ -116,6 +117,7 @@ _SIGS = {
     "LibShalom_set_splitk": (_I, [_I]),
     "LibShalom_set_tma": (_I, [_I]),
     "LibShalom_finalize": (None, []),
+    "LibShalom_selftest_wait_expiry": (_I, [_I]),
     "LibShalom_sgemm_batched": (_I, [_P, _L]),
     "LibShalom_sgemm_batched_strided": (_I, [_I, _L, _L, _L, _F, _P, _L, _P, _L, _F, _P, _L,
                                              _L]),
@@ -387,6 +389,12 @@ def set_tma(on: bool) -> None:
 
 def finalize() -> None:
     lib().LibShalom_finalize()
+
+
+def selftest_wait_expiry(iterations: int = 0) -> int:
+    """Runs the bounded-wait self-check kernel; returns its status
+    (ERR_DEVICE_TIMEOUT is the expected outcome)."""
+    return lib().LibShalom_selftest_wait_expiry(int(iterations))
 
 
 # --------------------------------------------------------------------------

@@ -575,6 +575,22 @@ static int defer_launch() {
   return finish_launch("defer_flush");
 }
 
+int flush_deferred() {
+  State &st = state();
+  if (st.ring_s_n == 0 && st.ring_d_n == 0) {
+    defer_sets().clear();
+    return LIBSHALOM_SUCCESS;
+  }
+  int cur = -1;
+  LS_CUDA_TRY(cudaGetDevice(&cur));
+  if (st.ring_device < 0 || cur == st.ring_device) return defer_launch();
+  // the pending calls name memory of the device they were recorded on
+  LS_CUDA_TRY(cudaSetDevice(st.ring_device));
+  const int rc = defer_launch();
+  LS_CUDA_TRY(cudaSetDevice(cur));
+  return rc;
+}
+
 // Largest call worth recording (M N K): the grouped kernels give each call to
 // one CTA, so a larger call runs faster directly, over many CTAs.
 constexpr double DEFER_MAX_MNK = 2097152.0;  // 128^3
@@ -597,6 +613,13 @@ static int defer_record(int transa, int transb, T *C, const T *A, const T *B, lo
     *status = LIBSHALOM_ERR_INVALID_VALUE;
     return 1;
   }
+  int rc = ensure_device();
+  if (!rc && st.ring_s_n + st.ring_d_n > 0 && st.device != st.ring_device)
+    rc = flush_deferred();  // calls recorded on another device run there first
+  if (rc) {
+    *status = rc;
+    return 1;
+  }
   DeferSets &ds = defer_sets();
   const bool fits = transa == NoTrans && (double)M * (double)N * (double)K <= DEFER_MAX_MNK;
   const bool waw_ok = C == ds.last_c && M == ds.last_m && N == ds.last_n;
@@ -604,14 +627,14 @@ static int defer_record(int transa, int transb, T *C, const T *A, const T *B, lo
                       (ds.writes.count(C) && !waw_ok);
   if (!fits || hazard) {
     // run (or start a new batch) after everything recorded so far
-    const int rc = defer_launch();
+    rc = defer_launch();
     if (rc) {
       *status = rc;
       return 1;
     }
     if (!fits) return 0;
   }
-  int rc = ring_idle();
+  rc = ring_idle();
   if (!rc) {
     if (sizeof(T) == 4) rc = ring_grow(&st.ring_s, &st.ring_s_cap, st.ring_s_n + 1);
     else rc = ring_grow(&st.ring_d, &st.ring_d_cap, st.ring_d_n + 1);
@@ -621,6 +644,7 @@ static int defer_record(int transa, int transb, T *C, const T *A, const T *B, lo
     return 1;
   }
   const int32_t ldb = (int32_t)(transb ? K : N);
+  if (st.ring_s_n + st.ring_d_n == 0) st.ring_device = st.device;
   if (sizeof(T) == 4) {
     LibShalom_sgemm_entry &e = st.ring_s[st.ring_s_n++];
     e.A = reinterpret_cast<const float *>(A);
@@ -647,10 +671,45 @@ static int defer_record(int transa, int transb, T *C, const T *A, const T *B, lo
   return 1;
 }
 
-// the drop-in calls: recorded while deferring, else run now
+// Operand classification of the drop-in calls.  The reference's callers pass
+// malloc'd HOST buffers to LibShalom_sgemm / _sgemm_mp / _dgemm (its
+// Hello.c:13-37 does exactly that); this library's drop-ins take device
+// memory.  A call whose operands include host memory (pageable or page-locked)
+// therefore runs through the host-memory pipeline of the _host calls instead
+// of handing host addresses to a kernel.  Device and managed memory run on
+// the device path.  Under unified addressing an address that was device
+// memory once stays a device address, so device pointers are remembered.
+static bool is_host_memory(const void *p) {
+  static const void *seen[32] = {};
+  static unsigned next = 0;
+  if (!p) return false;
+  for (const void *q : seen)
+    if (q == p) return false;
+  cudaPointerAttributes a;
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;  // not classifiable: left to the device path's own checks
+  }
+  if (a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged) {
+    seen[next++ % 32] = p;
+    return false;
+  }
+  return true;  // cudaMemoryTypeHost (page-locked) or cudaMemoryTypeUnregistered
+}
+
+// the drop-in calls: host operands through the host pipeline; recorded while
+// deferring; else run now
 template <typename T>
 static int dropin(int kind, int transa, int transb, T *C, const T *A, const T *B, long M,
                   long N, long K, bool mp) {
+  const bool args_ok = (transa == NoTrans || transa == Trans) &&
+                       (transb == NoTrans || transb == Trans) && M > 0 && N > 0 && K >= 0 &&
+                       C && (K == 0 || (A && B));
+  if (args_ok && ensure_device() == LIBSHALOM_SUCCESS &&
+      (is_host_memory(C) || (K > 0 && (is_host_memory(A) || is_host_memory(B))))) {
+    const int rc = flush_deferred();
+    return rc ? rc : gemm_host<T>(transa, transb, C, A, B, M, N, K, mp);
+  }
   if (state().deferring) {
     int status = LIBSHALOM_SUCCESS;
     if (defer_record<T>(transa, transb, C, A, B, M, N, K, &status) != 0) return status;
@@ -703,10 +762,14 @@ int LibShalom_defer_pending(void) {
   return (int)std::min(n, (long)INT32_MAX);
 }
 
+// The setters below change how later calls launch; calls still pending in a
+// deferred section are launched first, under the settings they were made with.
+
 void LibShalom_set_thread_nums(int num) {
   std::lock_guard<std::mutex> lk(state().mu);
-  state().thread_cap = num > 0 ? num : 0;
-  set_error(LIBSHALOM_SUCCESS);
+  const int rc = flush_deferred();
+  if (!rc) state().thread_cap = num > 0 ? num : 0;
+  set_error(rc);
 }
 
 void LibShalom_set_thread_ways(int tm, int tn) {
@@ -737,9 +800,23 @@ const char *LibShalom_error_string(int status) {
 
 int LibShalom_set_stream(void *stream) {
   std::lock_guard<std::mutex> lk(state().mu);
-  state().stream = reinterpret_cast<cudaStream_t>(stream);
-  set_error(LIBSHALOM_SUCCESS);
-  return LIBSHALOM_SUCCESS;
+  State &st = state();
+  const int rc = flush_deferred();
+  cudaStream_t next = reinterpret_cast<cudaStream_t>(stream);
+  if (!rc && next != st.stream) {
+    // The library's device buffers (workspace, front-end buffer, the copy of
+    // the deferred entries) are handed from call to call in stream order.
+    // Work queued on the old stream may still read them, so it is finished
+    // before calls on the new stream can overwrite them.  (A stream the
+    // caller has already destroyed reports an error here, which is ignored:
+    // its queued work completes anyway.)
+    if (st.ws || st.fe) {
+      if (cudaStreamSynchronize(st.stream) != cudaSuccess) cudaGetLastError();
+    }
+    st.stream = next;
+  }
+  set_error(rc);
+  return rc;
 }
 
 int LibShalom_set_sync(int synchronous) {
@@ -764,7 +841,7 @@ int LibShalom_set_precision(int mode) {
   if (mode != LIBSHALOM_PREC_FP32 && mode != LIBSHALOM_PREC_BF16X3 &&
       mode != LIBSHALOM_PREC_BF16X6)
     rc = LIBSHALOM_ERR_INVALID_VALUE;
-  else
+  else if (!(rc = flush_deferred()))
     state().precision = mode;
   set_error(rc);
   return rc;
@@ -780,7 +857,7 @@ int LibShalom_set_dgemm_method(int method, int slices) {
     rc = LIBSHALOM_ERR_INVALID_VALUE;
   else if (slices != 0 && (slices < 4 || slices > 9))
     rc = LIBSHALOM_ERR_INVALID_VALUE;
-  else {
+  else if (!(rc = flush_deferred())) {
     state().dgemm_method = method;
     state().ozaki_slices = slices == 0 ? 9 : slices;
   }
@@ -842,6 +919,8 @@ int LibShalom_set_tma(int enable) {
 void LibShalom_finalize(void) {
   std::lock_guard<std::mutex> lk(state().mu);
   State &st = state();
+  // calls still pending in a deferred section run before anything is freed
+  const int flushed = flush_deferred();
   if (st.ws || st.fe) cudaStreamSynchronize(st.stream);
   graph_cache_clear();
   if (st.ring_busy && st.ring_ev) cudaEventSynchronize(st.ring_ev);
@@ -870,7 +949,17 @@ void LibShalom_finalize(void) {
   st.fe = nullptr;
   st.fe_bytes = 0;
   st.fe_device = -1;
-  set_error(LIBSHALOM_SUCCESS);
+  st.ring_device = -1;
+  set_error(flushed);
+}
+
+int LibShalom_selftest_wait_expiry(int iterations) {
+  std::lock_guard<std::mutex> lk(state().mu);
+  int rc = iterations < 0 ? LIBSHALOM_ERR_INVALID_VALUE : flush_deferred();
+  if (!rc) rc = ensure_device();
+  if (!rc) rc = tc_wait_expiry_selftest(iterations);
+  set_error(rc);
+  return rc;
 }
 
 static bool entries_ok(const void *entries, long count) {
@@ -881,7 +970,7 @@ int LibShalom_sgemm_batched(const LibShalom_sgemm_entry *entries, long count) {
   std::lock_guard<std::mutex> lk(state().mu);
   int rc = LIBSHALOM_SUCCESS;
   if (!entries_ok(entries, count)) rc = LIBSHALOM_ERR_INVALID_VALUE;
-  else if (count > 0 && !(rc = ensure_device())) {
+  else if (count > 0 && !(rc = flush_deferred()) && !(rc = ensure_device())) {
     if (state().precision == LIBSHALOM_PREC_FP32) rc = run_grouped_s(entries, count);
     else rc = tc_sgemm_grouped(entries, count, state().precision);
     if (!rc) rc = finish_launch("sgemm_batched");
@@ -900,7 +989,7 @@ int LibShalom_sgemm_batched_strided(int transb, long M, long N, long K, float al
     rc = LIBSHALOM_ERR_INVALID_VALUE;
   else if (count > 0 && M > 0 && N > 0 && (!C || (K > 0 && (!A || !B))))
     rc = LIBSHALOM_ERR_INVALID_VALUE;
-  else if (count > 0 && M > 0 && N > 0 && !(rc = ensure_device())) {
+  else if (count > 0 && M > 0 && N > 0 && !(rc = flush_deferred()) && !(rc = ensure_device())) {
     GemmArgs<float> g;
     g.A = A; g.B = B; g.C = C;
     g.M = M; g.N = N; g.K = K;
@@ -930,7 +1019,7 @@ int LibShalom_sgemm_batched_strided_host(int transb, long M, long N, long K, flo
     rc = LIBSHALOM_ERR_INVALID_VALUE;  // the copies out would overlap
   else if (count > 0 && M > 0 && N > 0 && (!C || (K > 0 && (!A || !B))))
     rc = LIBSHALOM_ERR_INVALID_VALUE;
-  else if (count > 0 && M > 0 && N > 0 && !(rc = ensure_device())) {
+  else if (count > 0 && M > 0 && N > 0 && !(rc = flush_deferred()) && !(rc = ensure_device())) {
     const int prec = state().precision;
     auto compute = [&](float *dA, float *dB, float *dC, long dsA, long dsB, long dsC, long,
                        long n) {
@@ -961,26 +1050,32 @@ int LibShalom_sgemm_batched_strided_host(int transb, long M, long N, long K, flo
 void LibShalom_sgemm_host(int transa, int transb, float *C, const float *A, const float *B,
                           long M, long N, long K) {
   std::lock_guard<std::mutex> lk(state().mu);
-  set_error(gemm_host<float>(transa, transb, C, A, B, M, N, K, false));
+  int rc = flush_deferred();
+  if (!rc) rc = gemm_host<float>(transa, transb, C, A, B, M, N, K, false);
+  set_error(rc);
 }
 
 void LibShalom_sgemm_mp_host(int transa, int transb, float *C, const float *A, const float *B,
                              long M, long N, long K) {
   std::lock_guard<std::mutex> lk(state().mu);
-  set_error(gemm_host<float>(transa, transb, C, A, B, M, N, K, true));
+  int rc = flush_deferred();
+  if (!rc) rc = gemm_host<float>(transa, transb, C, A, B, M, N, K, true);
+  set_error(rc);
 }
 
 void LibShalom_dgemm_host(int transa, int transb, double *C, const double *A, const double *B,
                           long M, long N, long K) {
   std::lock_guard<std::mutex> lk(state().mu);
-  set_error(gemm_host<double>(transa, transb, C, A, B, M, N, K, false));
+  int rc = flush_deferred();
+  if (!rc) rc = gemm_host<double>(transa, transb, C, A, B, M, N, K, false);
+  set_error(rc);
 }
 
 int LibShalom_dgemm_batched(const LibShalom_dgemm_entry *entries, long count) {
   std::lock_guard<std::mutex> lk(state().mu);
   int rc = LIBSHALOM_SUCCESS;
   if (!entries_ok(entries, count)) rc = LIBSHALOM_ERR_INVALID_VALUE;
-  else if (count > 0 && !(rc = ensure_device())) {
+  else if (count > 0 && !(rc = flush_deferred()) && !(rc = ensure_device())) {
     const State &st = state();
     rc = st.dgemm_method == LIBSHALOM_DGEMM_FMA
              ? run_grouped_d(entries, count)
@@ -995,7 +1090,9 @@ int LibShalom_sgemm_ex(int transa, int transb, long M, long N, long K, float alp
                        const float *A, long lda, const float *B, long ldb, float beta, float *C,
                        long ldc) {
   std::lock_guard<std::mutex> lk(state().mu);
-  const int rc = gemm_common<float>(transa, transb, C, A, B, M, N, K, true, alpha, beta,
+  int rc = flush_deferred();
+  if (!rc)
+    rc = gemm_common<float>(transa, transb, C, A, B, M, N, K, true, alpha, beta,
                                     std::max(lda, 1L), std::max(ldb, 1L), std::max(ldc, 1L));
   set_error(rc);
   return rc;
@@ -1005,7 +1102,9 @@ int LibShalom_dgemm_ex(int transa, int transb, long M, long N, long K, double al
                        const double *A, long lda, const double *B, long ldb, double beta,
                        double *C, long ldc) {
   std::lock_guard<std::mutex> lk(state().mu);
-  const int rc = gemm_common<double>(transa, transb, C, A, B, M, N, K, true, alpha, beta,
+  int rc = flush_deferred();
+  if (!rc)
+    rc = gemm_common<double>(transa, transb, C, A, B, M, N, K, true, alpha, beta,
                                      std::max(lda, 1L), std::max(ldb, 1L), std::max(ldc, 1L));
   set_error(rc);
   return rc;
@@ -1020,7 +1119,7 @@ int LibShalom_dgemm_stack(const LibShalom_dgemm_stack_desc *stack, long count) {
                           (!stack->K && stack->k < 0)) ||
                          (stack->transb != NoTrans && stack->transb != Trans)))
     rc = LIBSHALOM_ERR_INVALID_VALUE;
-  else if (count > 0 && !(rc = ensure_device())) {
+  else if (count > 0 && !(rc = flush_deferred()) && !(rc = ensure_device())) {
     void *buf = nullptr;
     rc = frontend_buffer(sizeof(LibShalom_dgemm_entry) * (size_t)count, &buf);
     if (!rc) {
@@ -1058,11 +1157,11 @@ int LibShalom_sconv2d_nchw(const float *x, long n, long c, long h, long w, const
   // the implicit GEMM indexes k = (ci, r, q) and p = (oy, ox) in int32
   const bool small_idx = c * kh * kw < INT32_MAX && oh * ow < INT32_MAX && c * h * w < INT32_MAX;
   if (!rc && n > 0 && state().precision == LIBSHALOM_PREC_FP32 && small_idx &&
-      !(rc = ensure_device())) {
+      !(rc = flush_deferred()) && !(rc = ensure_device())) {
     // FP32: implicit GEMM, the tile loader gathers the im2col columns (no buffer)
     rc = conv_implicit(x, n, c, h, w, wt, oc, kh, kw, sh, sw, ph, pw, oh, ow, y);
     if (!rc) rc = finish_launch("sconv2d_nchw");
-  } else if (!rc && n > 0 && !(rc = ensure_device())) {
+  } else if (!rc && n > 0 && !(rc = flush_deferred()) && !(rc = ensure_device())) {
     const long K = c * kh * kw, P = oh * ow;
     void *buf = nullptr;
     rc = frontend_buffer(sizeof(float) * (size_t)K * P, &buf);

@@ -81,6 +81,7 @@ struct State {
   long ring_s_n = 0, ring_s_cap = 0, ring_d_n = 0, ring_d_cap = 0;
   cudaEvent_t ring_ev = nullptr;
   bool ring_busy = false;  // a flush's copies may still read the rings
+  int ring_device = -1;    // device current when the pending calls were recorded
 };
 
 State &state();
@@ -90,8 +91,14 @@ State &state();
 int ensure_device();
 
 // Device workspace of at least `bytes` bytes (grown on demand, stream
-// ordered: the caller's stream is synchronised before a regrow).
+// ordered: the caller's stream is synchronised before a regrow;
+// LibShalom_set_stream finishes the old stream's work before a switch).
 int workspace(size_t bytes, void **out);
+
+// Launches the drop-in calls recorded since LibShalom_defer_begin (on the
+// device that was current when they were recorded), so that whatever the
+// caller does next is ordered after them.  No-op when nothing is pending.
+int flush_deferred();
 
 // Number of CTAs to launch for `work_items` independent items of a kernel
 // with `per_sm` resident CTAs per SM, honouring LibShalom_set_thread_nums.

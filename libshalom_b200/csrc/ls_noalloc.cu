@@ -62,7 +62,9 @@ static int sgemm_mp_noalloc(int transa, int transb, float *C, const float *A, co
   if (M > (1L << 30) || N > (1L << 30) ||
       (double)splits * (double)M * (double)N > (double)LIBSHALOM_NOALLOC_SCRATCH_FLOATS)
     return LIBSHALOM_ERR_INVALID_VALUE;
-  int rc = ensure_device();
+  int rc = flush_deferred();  // ordered after pending deferred calls
+  if (rc) return rc;
+  rc = ensure_device();
   if (rc) return rc;
   float *scratch = nullptr;
   rc = noalloc_scratch(&scratch);

@@ -630,9 +630,10 @@ __device__ __forceinline__ void tma_load_3d(uint32_t dst, const CUtensorMap *map
 }
 
 // Bounded wait that also gives up as soon as another role has aborted.
+// `limit` polls (about a second with the default) before it gives up.
 __device__ __forceinline__ bool ws_wait(uint64_t *bar, uint32_t parity, volatile int *abort_flag,
-                                        unsigned *err) {
-  for (uint32_t it = 0; it < (1u << 22); ++it) {
+                                        unsigned *err, uint32_t limit = 1u << 22) {
+  for (uint32_t it = 0; it < limit; ++it) {
     if (ptx::mbar_try_wait(bar, parity)) return true;
     if ((it & 255) == 255 && *abort_flag) return false;
     if (it > 64) __nanosleep(it < 4096 ? 32 : 256);
@@ -1677,6 +1678,24 @@ __global__ void __launch_bounds__(G_THREADS, 1) k_tc_grouped(const GrpArgs g) {
 // device status word for the bounded waits
 __device__ unsigned g_tc_err;
 
+// Self-check of the bounded waits: an mbarrier nothing ever arrives at.  Warp
+// 0 polls it `limit` times, gives up, raises the abort flag and sets the
+// status word; warp 1 polls it with the kernels' full limit and gives up as
+// soon as it sees the abort flag -- the path by which every role of a
+// tensor-core kernel leaves after one role's wait has expired.
+__global__ void k_wait_expiry(uint32_t limit, unsigned *err) {
+  __shared__ uint64_t bar;
+  __shared__ int abort_flag;
+  if (threadIdx.x == 0) {
+    ptx::mbar_init(&bar, 1);
+    abort_flag = 0;
+    ptx::fence_mbar_init();
+  }
+  __syncthreads();
+  if (threadIdx.x < 32) ws_wait(&bar, 0, &abort_flag, err, limit);
+  else ws_wait(&bar, 0, &abort_flag, err);
+}
+
 // cuTensorMapEncodeTiled through the runtime's driver entry point (the
 // library does not link libcuda directly)
 PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
@@ -1918,6 +1937,23 @@ int tc_sgemm_single(const GemmArgs<float> &g, int mode, int splits, int *used) {
   rc = tc_launch(p, mode);
   if (rc) return rc;
   return run_splitk_reduce_f32(partial, s, g.M, g.N, g.C, g.ldc, g.alpha, g.beta);
+}
+
+int tc_wait_expiry_selftest(int iterations) {
+  State &st = state();
+  void *errp = nullptr;
+  LS_CUDA_TRY(cudaGetSymbolAddress(&errp, g_tc_err));
+  LS_CUDA_TRY(cudaStreamSynchronize(st.stream));  // no other kernel may own the word
+  LS_CUDA_TRY(cudaMemsetAsync(errp, 0, sizeof(unsigned), st.stream));
+  const uint32_t limit = iterations > 0 ? (uint32_t)std::min(iterations, 1 << 22) : 4096u;
+  k_wait_expiry<<<1, 64, 0, st.stream>>>(limit, reinterpret_cast<unsigned *>(errp));
+  LS_CUDA_TRY(cudaGetLastError());
+  LS_CUDA_TRY(cudaStreamSynchronize(st.stream));
+  unsigned err = 0;
+  LS_CUDA_TRY(cudaMemcpyFromSymbol(&err, g_tc_err, sizeof(err)));
+  const unsigned zero = 0;
+  LS_CUDA_TRY(cudaMemcpyToSymbol(g_tc_err, &zero, sizeof(zero)));
+  return err ? LIBSHALOM_ERR_DEVICE_TIMEOUT : LIBSHALOM_SUCCESS;
 }
 
 int tc_sgemm_grouped(const LibShalom_sgemm_entry *entries, long count, int mode) {

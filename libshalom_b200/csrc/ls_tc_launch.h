@@ -18,4 +18,8 @@ int tc_sgemm_strided(const GemmArgs<float> &g, long sA, long sB, long sC, long c
 // Grouped batch (entries in device memory) on the tensor cores.
 int tc_sgemm_grouped(const LibShalom_sgemm_entry *entries, long count, int mode);
 
+// Runs the bounded-wait self-check kernel (an mbarrier nothing arrives at);
+// returns LIBSHALOM_ERR_DEVICE_TIMEOUT when its waits expired and reported.
+int tc_wait_expiry_selftest(int iterations);
+
 }  // namespace ls

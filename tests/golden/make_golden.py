@@ -8,8 +8,8 @@ with inputs from the reference benchmarks' own generator (random_matrix():
 srand48(seed), a = 2.0*(float)drand48() - 1.0; restated bit-exactly in
 oracle/oracle.c and checked against glibc), and stores the outputs.
 
-Run here, where the reference source is mounted:
-    python tests/golden/make_golden.py /root/reference
+Run where the reference source is checked out:
+    python tests/golden/make_golden.py <reference checkout>
 Nothing at test or bench time reads the reference; the tests regenerate the
 inputs from the stored seeds and compare against the stored outputs.
 
@@ -110,4 +110,6 @@ def main(ref_root):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        sys.exit("usage: make_golden.py <path of the reference checkout>")
+    main(sys.argv[1])

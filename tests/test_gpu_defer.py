@@ -151,3 +151,62 @@ def test_deferred_split_bf16_on_a_side_stream(reset):
     ls.synchronize()
     for (_, tb, M, N, K, A, B), C in zip(probs, outs):
         assert normwise_err(to_host(C), orc.sgemm_f64(A, B, tb)) <= 1e-6
+
+
+def _entries(sdt, rows):
+    """Device buffer of SgemmEntry records: rows of (A, B, C, M, N, K, transb)."""
+    ent = np.array([(a.data_ptr(), b.data_ptr(), c.data_ptr(), M, N, K, tb, 0, 0, 0, 1.0, 0.0, 0)
+                    for (a, b, c, M, N, K, tb) in rows], sdt)
+    return to_dev(ent.view(np.uint8))
+
+
+def test_batched_and_ex_calls_run_after_pending_calls(reset):
+    """Calls that are not recorded (a grouped batch, an _ex call) read a C that
+    a pending recorded call writes: they must launch the pending calls first."""
+    import torch
+    n = 20
+    A, B = orc.gemm_inputs_f32(21, n, n, n, 0)
+    D = orc.uniform_f32(22, n * n).reshape(n, n)
+    dA, dB, dD = to_dev(A), to_dev(B), to_dev(D)
+    X = torch.full((n, n), float("nan"), device="cuda")
+    Y = torch.full((n, n), float("nan"), device="cuda")
+    Z = torch.full((n, n), float("nan"), device="cuda")
+    sdt, _ = ls.entry_dtypes()
+    ent = _entries(sdt, [(X, dD, Y, n, n, n, 0)])  # Y = X D
+    ls.defer_begin()
+    ls.sgemm(0, 0, X, dA, dB, n, n, n)  # recorded: X = A B
+    assert ls.defer_pending() == 1
+    ls.sgemm_batched(ent, 1)            # reads X: the recorded call runs first
+    assert ls.defer_pending() == 0
+    ls.sgemm(0, 0, X, dA, dB, n, n, n)  # recorded again
+    ls.sgemm_ex(0, 0, n, n, n, 1.0, X, n, dD, n, 0.0, Z, n)  # Z = X D, after the pending call
+    assert ls.defer_pending() == 0
+    ls.defer_flush()
+    x = orc.sgemm_kseq(A, B, 0)
+    assert np.array_equal(to_host(X), x)
+    assert normwise_err(to_host(Y), orc.sgemm_f64(x, D, 0)) <= 1e-6
+    assert normwise_err(to_host(Z), orc.sgemm_f64(x, D, 0)) <= 1e-6
+
+
+def test_setters_and_finalize_launch_pending_calls(reset):
+    """Changing the precision launches the pending calls under the precision
+    they were recorded with; finalize runs what is still pending."""
+    import torch
+    A, B = orc.gemm_inputs_f32(23, 33, 17, 29, 0)
+    dA, dB = to_dev(A), to_dev(B)
+    C1 = torch.full((33, 17), float("nan"), device="cuda")
+    C2 = torch.full((33, 17), float("nan"), device="cuda")
+    ls.defer_begin()
+    ls.sgemm_mp(0, 0, C1, dA, dB, 33, 17, 29)   # recorded under plain FP32
+    ls.set_precision(ls.PREC_BF16X6)           # launches it first
+    assert ls.defer_pending() == 0
+    ls.set_precision(ls.PREC_FP32)
+    ls.sgemm(0, 0, C2, dA, dB, 33, 17, 29)
+    assert ls.defer_pending() == 1
+    ls.finalize()                              # runs the pending call, then frees
+    assert ls.last_error() == ls.SUCCESS
+    assert ls.defer_pending() == 0
+    torch.cuda.synchronize()
+    ref = orc.sgemm_kseq(A, B, 0)
+    assert np.array_equal(to_host(C1), ref)  # plain FP32 result, bit for bit
+    assert np.array_equal(to_host(C2), ref)
