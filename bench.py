@@ -62,6 +62,8 @@ def parse():
     p.add_argument("--mode", default="auto", choices=["auto", "fp32", "bf16x3", "bf16x6"])
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu", action="store_true")
+    p.add_argument("--no-secondary", action="store_true",
+                   help="skip the mixed, DGEMM-run and irregular workloads of the default run")
     p.add_argument("--workload", default="cube-sweep",
                    choices=["cube-sweep", "single", "irregular", "dgemm-runs", "mixed"],
                    help="cube-sweep is the headline; the others measure the other shapes")
@@ -403,6 +405,23 @@ def run_gpu(args):
                           f"of the reference's 5x16-tile algorithm (AArch64 NEON assembly not "
                           f"buildable on x86), OpenMP over GEMMs on {model}")}
 
+    # the other configurations, each device-timed over about a second with
+    # its own clock record, roofline, error and CPU baseline (one GPU only)
+    secondary = None
+    n_calls = len(bufs)
+    if world == 1 and not args.no_secondary:
+        bufs.clear()  # the sweep's 23 GB of device buffers (and pinned copies)
+        if e2e is not None:
+            host.clear()
+        torch.cuda.empty_cache()
+        secondary = {}
+        with torch.cuda.stream(stream):
+            for key, fn in (("mixed", measure_mixed), ("dgemm_runs", measure_dgemm_runs),
+                            ("irregular", measure_irregular)):
+                secondary[key] = fn(args, torch, ls, stream, cpu=not args.no_cpu)
+                torch.cuda.empty_cache()
+        ls.set_precision(ls.PREC_FP32)
+
     names = {ls.PREC_FP32: "fp32", ls.PREC_BF16X3: "bf16x3", ls.PREC_BF16X6: "bf16x6"}
     line = {
         "metric": METRIC, "value": value, "unit": "GFLOP/s", "n_gpus": world,
@@ -423,7 +442,7 @@ def run_gpu(args):
                      # kernel on a 2000-GEMM n=128 capture (0.910 per algorithmic byte,
                      # profiles/k_tc_ws_bf16x6_nn128_batch2000.md), scaled to the
                      # average launch of this sweep
-                     "traffic": (TRAFFIC_PER_ALG_BYTE * step_bytes() / len(bufs)
+                     "traffic": (TRAFFIC_PER_ALG_BYTE * step_bytes() / n_calls
                                  if best == ls.PREC_BF16X6 else None),
                      "traffic_unit": "bytes per launch",
                      "peak_source": peak_src,
@@ -433,6 +452,7 @@ def run_gpu(args):
         "clocks": clk,
         "e2e": e2e,
         "cpu_baseline": cpu,
+        "workloads": secondary,
     }
     if rank == 0:
         print(json.dumps(line), flush=True)
@@ -563,56 +583,172 @@ def wl_single(args):
 
 IRREGULAR = [(64, 3136, 576), (128, 784, 1152), (256, 196, 2304), (512, 49, 4608),
              (20480, 32, 20480), (32, 20480, 4096)]
-
-
-def wl_irregular(args):
-    """LibShalom_sgemm_mp on the six tall-skinny / im2col shapes, NN."""
-    torch, ls, s = _gpu_setup()
-    g = torch.Generator(device="cuda")
-    g.manual_seed(3)
-    bufs = []
-    for (M, N, K) in IRREGULAR:
-        A = torch.rand((M, K), generator=g, device="cuda") * 2 - 1
-        B = torch.rand((K, N), generator=g, device="cuda") * 2 - 1
-        bufs.append((M, N, K, A, B, torch.empty((M, N), device="cuda")))
-    res = {}
-    modes = {"fp32_splitk_auto": (ls.PREC_FP32, 0), "fp32_reference_order": (ls.PREC_FP32, 1),
-             "bf16x6": (ls.PREC_BF16X6, 0), "bf16x3": (ls.PREC_BF16X3, 0)}
-    for name, (prec, split) in modes.items():
-        ls.set_precision(prec)
-        ls.set_splitk(split)
-        per = {}
-        tot_ms = 0.0
-        for (M, N, K, A, B, C) in bufs:
-            ms = _time_events(torch, s, lambda: ls.sgemm_mp(0, 0, C, A, B, M, N, K),
-                              args.steps, args.warmup)
-            ref = A.double() @ B.double()
-            err = ((C.double() - ref).abs().max() / ref.abs().max()).item()
-            per[f"{M}x{N}x{K}"] = {"ms": ms, "gflops": 2.0 * M * N * K / (ms / 1e3) / 1e9,
-                                   "max_normwise_err": err}
-            tot_ms += ms
-        flops = sum(2.0 * M * N * K for (M, N, K) in IRREGULAR)
-        res[name] = {"gflops": flops / (tot_ms / 1e3) / 1e9, "ms_all_shapes": tot_ms,
-                     "shapes": per}
-    ls.set_precision(ls.PREC_FP32)
-    ls.set_splitk(0)
-    ok = {k: v for k, v in res.items()
-          if max(x["max_normwise_err"] for x in v["shapes"].values()) <= 1e-6}
-    best = max(ok, key=lambda k: ok[k]["gflops"])
-    alg_bytes = sum(4.0 * (M * K + K * N + M * N) for (M, N, K) in IRREGULAR)
-    _emit("irregular SGEMM (sgemm_mp) aggregate GFLOP/s over the six shapes",
-          res[best]["gflops"], "GFLOP/s", res[best]["ms_all_shapes"], args,
-          {"workload": "LibShalom_sgemm_mp NN on (64,3136,576) (128,784,1152) (256,196,2304) "
-                       "(512,49,4608) (20480,32,20480) (32,20480,4096)", "mode": best},
-          alg_bytes, {"dtype": "f32", "modes": res, "gpu_launches": None})
-
-
 DGEMM_SIZES = [5, 9, 13, 16, 22, 23, 26, 32]
 
 
-def wl_dgemm_runs(args, count=200_000, run=8):
-    """LibShalom_dgemm_batched: C += A B, runs of 8 products share C."""
-    torch, ls, s = _gpu_setup()
+def _graph(torch, s, fn):
+    """fn's launches captured into one CUDA graph on stream s (fn has already
+    run once, so every library buffer it needs exists)."""
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g, stream=s):
+        fn()
+    s.synchronize()
+    return g
+
+
+def _timed_with_clocks(torch, s, fn, args, min_ms=800.0):
+    """Average ms of fn over at least args.steps calls and about min_ms of
+    device time, with nvidia-smi clocks sampled over that region."""
+    est = _time_events(torch, s, fn, 2, args.warmup)
+    reps = max(args.steps, int(min_ms / max(est, 1e-3)) + 1)
+    clocks = Clocks(torch.cuda.current_device())
+    clocks.start()
+    time.sleep(0.3)
+    ms = _time_events(torch, s, fn, reps, 1)
+    return ms, reps, clocks.stop()
+
+
+def _roofline(alg_bytes, ms, kernel):
+    peak, src = _peak_hbm()
+    gbs = alg_bytes / (ms / 1e3) / 1e9
+    return {"bound": "hbm", "achieved": gbs, "peak": peak, "unit": "GB/s", "frac": gbs / peak,
+            "traffic": None, "peak_source": src, "kernel": kernel}
+
+
+def _cpu_desc(what, threads):
+    model, _ = cpu_info()
+    return (f"{what}; C restatement of the reference's algorithm (AArch64 NEON assembly not "
+            f"buildable on x86), OpenMP over GEMMs, {threads} threads on {model}")
+
+
+def _cpu_timed(fn, target_s=4.0, start=500, cap=None):
+    """Times fn(n) on growing n until one call takes about target_s; returns
+    (seconds, n).  fn(n) runs the CPU port on the first n units."""
+    n = start
+    while True:
+        t0 = time.perf_counter()
+        fn(n)
+        dt = time.perf_counter() - t0
+        if dt >= target_s * 0.5 or (cap is not None and n >= cap):
+            return dt, n
+        n = int(n * min(8.0, max(2.0, target_s / max(dt, 1e-3))))
+        if cap is not None:
+            n = min(n, cap)
+
+
+def measure_mixed(args, torch, ls, s, count=50_000, cpu=True):
+    """LibShalom_sgemm_batched on 50,000 GEMMs, M, N, K log-uniform integers
+    in [4, 256], NN/NT 50/50, alpha 1, beta 0/1, one captured CUDA graph."""
+    rng = np.random.default_rng(5)
+    dims = np.exp(rng.uniform(np.log(4), np.log(256), size=(count, 3))).astype(np.int64)
+    M, N, K = dims[:, 0], dims[:, 1], dims[:, 2]
+    tb = rng.integers(2, size=count)
+    beta = rng.integers(2, size=count).astype(np.float32)
+    a_len, b_len, c_len = M * K, K * N, M * N
+    offs = [np.concatenate([[0], np.cumsum(x)[:-1]]) for x in (a_len, b_len, c_len)]
+    g = torch.Generator(device="cuda")
+    g.manual_seed(13)
+    dA = torch.rand(int(a_len.sum()), generator=g, device="cuda") * 2 - 1
+    dB = torch.rand(int(b_len.sum()), generator=g, device="cuda") * 2 - 1
+    dC0 = torch.rand(int(c_len.sum()), generator=g, device="cuda") * 2 - 1
+    dC = dC0.clone()
+    sdt, _ = ls.entry_dtypes()
+    ent = np.zeros(count, sdt)
+    ent["A"] = dA.data_ptr() + 4 * offs[0]
+    ent["B"] = dB.data_ptr() + 4 * offs[1]
+    ent["C"] = dC.data_ptr() + 4 * offs[2]
+    ent["M"], ent["N"], ent["K"], ent["transb"] = M, N, K, tb
+    ent["alpha"] = 1.0
+    ent["beta"] = beta
+    dE = torch.from_numpy(ent.view(np.uint8)).cuda()
+    flops = float(2.0 * (M * N * K).sum())
+    alg_bytes = float(4.0 * (a_len.sum() + b_len.sum() + (c_len * (1 + beta)).sum()))
+    samp = np.linspace(0, count - 1, 250).astype(np.int64)
+
+    def sample_error():
+        err = 0.0
+        for i in samp:
+            a = dA[offs[0][i]:offs[0][i] + a_len[i]].double().view(int(M[i]), int(K[i]))
+            bb = dB[offs[1][i]:offs[1][i] + b_len[i]].double()
+            bm = bb.view(int(N[i]), int(K[i])).t() if tb[i] else bb.view(int(K[i]), int(N[i]))
+            ref = a @ bm + float(beta[i]) * dC0[offs[2][i]:offs[2][i] + c_len[i]].double().view(
+                int(M[i]), int(N[i]))
+            got = dC[offs[2][i]:offs[2][i] + c_len[i]].double().view(int(M[i]), int(N[i]))
+            e = ((got - ref).abs().max() / ref.abs().max()).item()
+            err = e if not (e <= err) else err  # NaN propagates
+        return err
+
+    modes = {}
+    for name, prec in (("bf16x3", ls.PREC_BF16X3), ("fp32", ls.PREC_FP32),
+                       ("bf16x6", ls.PREC_BF16X6)):
+        ls.set_precision(prec)
+        dC.copy_(dC0)
+        ls.sgemm_batched(dE, count)
+        s.synchronize()
+        err = sample_error()
+        graph = _graph(torch, s, lambda: ls.sgemm_batched(dE, count))
+        ms, reps, clk = _timed_with_clocks(torch, s, graph.replay, args)
+        del graph
+        modes[name] = {"gflops": flops / (ms / 1e3) / 1e9, "ms": ms, "max_normwise_err": err,
+                       "timed_replays": reps, "clocks": clk}
+    ls.set_precision(ls.PREC_FP32)
+    # looping plain FP32 per-call kernels over a sample, captured in one graph
+    # (the loop's launches replayed back to back: no host overhead timed)
+    sample = 5000
+
+    def percall():
+        for i in range(sample):
+            ls.sgemm_batched_strided(int(tb[i]), int(M[i]), int(N[i]), int(K[i]), 1.0,
+                                     dA.data_ptr() + 4 * int(offs[0][i]), 0,
+                                     dB.data_ptr() + 4 * int(offs[1][i]), 0, float(beta[i]),
+                                     dC.data_ptr() + 4 * int(offs[2][i]), 0, 1)
+    percall()
+    pg = _graph(torch, s, percall)
+    ms_pc = _time_events(torch, s, pg.replay, 3, 1)
+    del pg
+    pc_flops = float(2.0 * (M[:sample] * N[:sample] * K[:sample]).sum())
+    per_call = {"gflops": pc_flops / (ms_pc / 1e3) / 1e9, "sample_gemms": sample,
+                "how": "LibShalom_sgemm_batched_strided (plain FP32) once per GEMM, the "
+                       "calls captured in one CUDA graph and replayed"}
+    best = "bf16x6"
+    out = {"metric": "mixed uneven SGEMM batch GFLOP/s (50,000 GEMMs, log-uniform 4..256)",
+           "value": modes[best]["gflops"], "unit": "GFLOP/s", "ms_per_step": modes[best]["ms"],
+           "mode": best, "max_normwise_err": modes[best]["max_normwise_err"],
+           "config": {"workload": "LibShalom_sgemm_batched, M,N,K log-uniform integers in "
+                                  "[4,256], NN/NT 50/50, alpha 1, beta 0/1, one CUDA-graph "
+                                  "launch per step", "gemms": count,
+                      "step_gflop": flops / 1e9, "step_gbytes": alg_bytes / 1e9,
+                      "l2": "inputs larger than L2: 2.5 GB touched per step"},
+           "roofline": _roofline(alg_bytes, modes[best]["ms"], "sgemm grouped (bf16x6)"),
+           "clocks": modes[best]["clocks"], "modes": modes, "per_call_fp32": per_call,
+           "speedup_vs_per_call": modes[best]["gflops"] / per_call["gflops"],
+           "gpu_launches_per_step": 4}
+    if cpu:
+        from oracle import oracle as orc
+        threads = orc.max_threads()
+        n_host = min(count, 20000)
+        hA = dA[:int(offs[0][n_host - 1] + a_len[n_host - 1])].cpu().numpy()
+        hB = dB[:int(offs[1][n_host - 1] + b_len[n_host - 1])].cpu().numpy()
+        hC = dC0[:int(offs[2][n_host - 1] + c_len[n_host - 1])].cpu().numpy().copy()
+        i32 = lambda x: np.ascontiguousarray(x, np.int32)  # noqa: E731
+        i64 = lambda x: np.ascontiguousarray(x, np.int64)  # noqa: E731
+
+        def run(n):
+            orc.lib().orc_port_sgemm_batched(n, i32(M[:n]), i32(N[:n]), i32(K[:n]), i32(tb[:n]),
+                                             np.ascontiguousarray(beta[:n]), hA, i64(offs[0][:n]),
+                                             hB, i64(offs[1][:n]), hC, i64(offs[2][:n]), threads)
+        dt, n = _cpu_timed(run, cap=n_host)
+        f = float(2.0 * (M[:n] * N[:n] * K[:n]).sum())
+        out["cpu_baseline"] = {"value": f / dt / 1e9, "unit": "GFLOP/s", "cores": threads,
+                               "kind": "port",
+                               "sample": _cpu_desc(f"first {n} GEMMs of the batch "
+                                                   f"({f / 1e9:.2f} GFLOP in {dt:.2f} s)", threads)}
+    return out
+
+
+def measure_dgemm_runs(args, torch, ls, s, count=200_000, run=8, cpu=True):
+    """LibShalom_dgemm_batched: C += A B, runs of 8 products share C, one
+    captured CUDA graph per step."""
     rng = np.random.default_rng(7)
     nruns = count // run
     sz = np.array(DGEMM_SIZES)
@@ -647,11 +783,11 @@ def wl_dgemm_runs(args, count=200_000, run=8):
     dE = torch.from_numpy(ent.view(np.uint8)).cuda()
     flops = float(2.0 * (M * N * K).sum())
     alg_bytes = float(8.0 * (a_len.sum() + b_len.sum() + 2 * c_len.sum()))
-    # max normwise error per C block over a sample of runs, against torch FP64
-    # applied product by product on the GPU (C0 + sum of the run's products)
     samp = rng.choice(nruns, size=min(nruns, 300), replace=False)
 
     def run_error():
+        # max normwise error per C block over a sample of runs, against torch
+        # FP64 applied product by product on the GPU (C0 + the run's products)
         err = 0.0
         for r in samp:
             i0 = int(r) * run
@@ -667,21 +803,23 @@ def wl_dgemm_runs(args, count=200_000, run=8):
         return err
 
     methods = {}
-    for name, meth, sl in (("fma", ls.DGEMM_FMA, 0), ("dmma", ls.DGEMM_DMMA, 0),
-                           ("ozaki9", ls.DGEMM_OZAKI, 9), ("ozaki8", ls.DGEMM_OZAKI, 8)):
+    for name, meth, sl in (("fma", ls.DGEMM_FMA, 0), ("ozaki9", ls.DGEMM_OZAKI, 9),
+                           ("dmma", ls.DGEMM_DMMA, 0)):
         ls.set_dgemm_method(meth, sl)
         dC.copy_(dC0)
         ls.dgemm_batched(dE, count)
         s.synchronize()
         err = run_error()
-        mms = _time_events(torch, s, lambda: ls.dgemm_batched(dE, count), args.steps, args.warmup)
-        methods[name] = {"gflops": flops / (mms / 1e3) / 1e9, "ms": mms, "max_normwise_err": err,
-                         "gbs": alg_bytes / (mms / 1e3) / 1e9}
+        graph = _graph(torch, s, lambda: ls.dgemm_batched(dE, count))
+        ms, reps, clk = _timed_with_clocks(torch, s, graph.replay, args)
+        del graph
+        methods[name] = {"gflops": flops / (ms / 1e3) / 1e9, "ms": ms, "max_normwise_err": err,
+                         "gbs": alg_bytes / (ms / 1e3) / 1e9, "timed_replays": reps,
+                         "clocks": clk}
     ls.set_dgemm_method(ls.DGEMM_FMA, 0)
     ok = {k: v for k, v in methods.items() if v["max_normwise_err"] <= 1e-14}
     best = min(ok, key=lambda k: ok[k]["ms"]) if ok else "fma"
-    ms = methods[best]["ms"]
-    # per-call plain FP64 kernel over a sample of the same products
+    # per-call plain FP64 kernel over a sample of the products, in one graph
     sample = 4000
     C1 = dC.clone()
 
@@ -689,100 +827,148 @@ def wl_dgemm_runs(args, count=200_000, run=8):
         for i in range(sample):
             ls.dgemm(0, 0, C1.data_ptr() + 8 * int(offC[i]), dA.data_ptr() + 8 * int(offA[i]),
                      dB.data_ptr() + 8 * int(offB[i]), int(M[i]), int(N[i]), int(K[i]))
-    ms_pc = _time_events(torch, s, percall, 1, 1)
-    pc_gflops = float(2.0 * (M[:sample] * N[:sample] * K[:sample]).sum()) / (ms_pc / 1e3) / 1e9
-    value = flops / (ms / 1e3) / 1e9
-    _emit("batched uneven DGEMM GFLOP/s (200,000 products, runs of 8 share C)", value, "GFLOP/s",
-          ms, args,
-          {"workload": "LibShalom_dgemm_batched, C += A B, M,N per run and K per product from "
-                       "{5,9,13,16,22,23,26,32}, entries normal(0,1)*10^u, u~U[-3,3] per matrix",
-           "products": count, "run": run, "method": best,
-           "step_gflop": flops / 1e9, "step_gbytes": alg_bytes / 1e9},
-          alg_bytes,
-          {"dtype": "f64", "gpu_launches": 3 * args.steps, "methods": methods,
-           "per_call_plain_fp64": {"gflops": pc_gflops, "sample_products": sample,
-                                   "note": "loop of LibShalom_dgemm (overwrite semantics) on the "
-                                           "first products, stream-ordered"},
-           "speedup_vs_per_call": value / pc_gflops})
+    percall()
+    pg = _graph(torch, s, percall)
+    ms_pc = _time_events(torch, s, pg.replay, 3, 1)
+    del pg
+    pc_flops = float(2.0 * (M[:sample] * N[:sample] * K[:sample]).sum())
+    per_call = {"gflops": pc_flops / (ms_pc / 1e3) / 1e9, "sample_products": sample,
+                "how": "LibShalom_dgemm (plain FP64, overwrite semantics) once per product, "
+                       "the calls captured in one CUDA graph and replayed"}
+    value = methods[best]["gflops"]
+    out = {"metric": "batched uneven DGEMM GFLOP/s (200,000 products, runs of 8 share C)",
+           "value": value, "unit": "GFLOP/s", "ms_per_step": methods[best]["ms"],
+           "method": best, "max_normwise_err": methods[best]["max_normwise_err"],
+           "config": {"workload": "LibShalom_dgemm_batched, C += A B, M,N per run and K per "
+                                  "product from {5,9,13,16,22,23,26,32}, entries "
+                                  "normal(0,1)*10^u, u~U[-3,3] per matrix, one CUDA-graph "
+                                  "launch per step", "products": count, "run": run,
+                      "step_gflop": flops / 1e9, "step_gbytes": alg_bytes / 1e9,
+                      "l2": "inputs larger than L2: 1.2 GB touched per step"},
+           "roofline": _roofline(alg_bytes, methods[best]["ms"], f"dgemm grouped ({best})"),
+           "clocks": methods[best]["clocks"], "methods": methods,
+           "per_call_fp64": per_call, "speedup_vs_per_call": value / per_call["gflops"],
+           "gpu_launches_per_step": 2}
+    if cpu:
+        from oracle import oracle as orc
+        threads = orc.max_threads()
+        n_host = min(count, 40000)
+        hA = dA[:int(offA[n_host - 1] + a_len[n_host - 1])].cpu().numpy()
+        hB = dB[:int(offB[n_host - 1] + b_len[n_host - 1])].cpu().numpy()
+        hC = dC0[:int(offC[n_host - 1] + Mr[(n_host - 1) // run] * Nr[(n_host - 1) // run])]
+        hC = hC.cpu().numpy().copy()
+        i32 = lambda x: np.ascontiguousarray(x, np.int32)  # noqa: E731
+        i64 = lambda x: np.ascontiguousarray(x, np.int64)  # noqa: E731
+
+        def runc(n):
+            n = n // run * run
+            orc.lib().orc_port_dgemm_batched(n, i32(M[:n]), i32(N[:n]), i32(K[:n]), hA,
+                                             i64(offA[:n]), hB, i64(offB[:n]), hC,
+                                             i64(offC[:n]), threads)
+        dt, n = _cpu_timed(runc, start=800, cap=n_host)
+        n = n // run * run
+        f = float(2.0 * (M[:n] * N[:n] * K[:n]).sum())
+        out["cpu_baseline"] = {"value": f / dt / 1e9, "unit": "GFLOP/s", "cores": threads,
+                               "kind": "port",
+                               "sample": _cpu_desc(f"first {n} products ({n // run} runs, "
+                                                   f"{f / 1e9:.3f} GFLOP in {dt:.2f} s), 7x6 "
+                                                   f"FP64 tile", threads)}
+    return out
 
 
-def wl_mixed(args, count=50_000):
-    """LibShalom_sgemm_batched: log-uniform M, N, K in [4, 256], NN/NT, beta 0/1."""
-    torch, ls, s = _gpu_setup()
-    rng = np.random.default_rng(5)
-    dims = np.exp(rng.uniform(np.log(4), np.log(256), size=(count, 3))).astype(np.int64)
-    M, N, K = dims[:, 0], dims[:, 1], dims[:, 2]
-    tb = rng.integers(2, size=count)
-    beta = rng.integers(2, size=count).astype(np.float32)
-    a_len, b_len, c_len = M * K, K * N, M * N
-    offs = [np.concatenate([[0], np.cumsum(x)[:-1]]) for x in (a_len, b_len, c_len)]
+def measure_irregular(args, torch, ls, s, cpu=True):
+    """LibShalom_sgemm_mp on the six tall-skinny / im2col shapes, NN."""
     g = torch.Generator(device="cuda")
-    g.manual_seed(13)
-    dA = torch.rand(int(a_len.sum()), generator=g, device="cuda") * 2 - 1
-    dB = torch.rand(int(b_len.sum()), generator=g, device="cuda") * 2 - 1
-    dC0 = torch.rand(int(c_len.sum()), generator=g, device="cuda") * 2 - 1
-    dC = dC0.clone()
-    sdt, _ = ls.entry_dtypes()
-    ent = np.zeros(count, sdt)
-    ent["A"] = dA.data_ptr() + 4 * offs[0]
-    ent["B"] = dB.data_ptr() + 4 * offs[1]
-    ent["C"] = dC.data_ptr() + 4 * offs[2]
-    ent["M"], ent["N"], ent["K"], ent["transb"] = M, N, K, tb
-    ent["alpha"] = 1.0
-    ent["beta"] = beta
-    dE = torch.from_numpy(ent.view(np.uint8)).cuda()
-    flops = float(2.0 * (M * N * K).sum())
-    alg_bytes = float(4.0 * (a_len.sum() + b_len.sum() + (c_len * (1 + beta)).sum()))
+    g.manual_seed(3)
+    bufs = []
+    for (M, N, K) in IRREGULAR:
+        A = torch.rand((M, K), generator=g, device="cuda") * 2 - 1
+        B = torch.rand((K, N), generator=g, device="cuda") * 2 - 1
+        bufs.append((M, N, K, A, B, torch.empty((M, N), device="cuda")))
     res = {}
-    for name, prec in (("bf16x6", ls.PREC_BF16X6), ("bf16x3", ls.PREC_BF16X3),
-                       ("fp32", ls.PREC_FP32)):
+    modes = {"fp32_splitk_auto": (ls.PREC_FP32, 0), "fp32_reference_order": (ls.PREC_FP32, 1),
+             "bf16x3": (ls.PREC_BF16X3, 0), "bf16x6": (ls.PREC_BF16X6, 0)}
+    for name, (prec, split) in modes.items():
         ls.set_precision(prec)
-        dC.copy_(dC0)
-        ls.sgemm_batched(dE, count)
-        s.synchronize()
-        # error on a sample against FP64 (beta applied to the original C)
-        err = 0.0
-        for i in range(0, count, count // 200):
-            a = dA[offs[0][i]:offs[0][i] + a_len[i]].double().view(int(M[i]), int(K[i]))
-            bb = dB[offs[1][i]:offs[1][i] + b_len[i]].double()
-            bm = bb.view(int(N[i]), int(K[i])).t() if tb[i] else bb.view(int(K[i]), int(N[i]))
-            ref = a @ bm + float(beta[i]) * dC0[offs[2][i]:offs[2][i] + c_len[i]].double().view(
-                int(M[i]), int(N[i]))
-            got = dC[offs[2][i]:offs[2][i] + c_len[i]].double().view(int(M[i]), int(N[i]))
-            e = ((got - ref).abs().max() / ref.abs().max()).item()
-            err = e if not (e <= err) else err  # NaN propagates
-        ms = _time_events(torch, s, lambda: ls.sgemm_batched(dE, count), args.steps, args.warmup)
-        res[name] = {"gflops": flops / (ms / 1e3) / 1e9, "ms": ms, "max_normwise_err": err}
-    # the same batch replayed from a captured CUDA graph
-    ls.set_precision(ls.PREC_BF16X6)
-    graph = torch.cuda.CUDAGraph()
-    with torch.cuda.graph(graph, stream=s):
-        ls.sgemm_batched(dE, count)
-    ms_graph = _time_events(torch, s, graph.replay, args.steps, args.warmup)
-    res["bf16x6_graph"] = {"gflops": flops / (ms_graph / 1e3) / 1e9, "ms": ms_graph}
-    # looping plain FP32 per-call kernels over a sample
-    sample = 5000
-    ls.set_precision(ls.PREC_FP32)
+        ls.set_splitk(split)
+        per = {}
+        for (M, N, K, A, B, C) in bufs:
+            ls.sgemm_mp(0, 0, C, A, B, M, N, K)
+            s.synchronize()
+            ref = A.double() @ B.double()
+            err = ((C.double() - ref).abs().max() / ref.abs().max()).item()
+            per[f"{M}x{N}x{K}"] = {"max_normwise_err": err}
 
-    def percall():
-        for i in range(sample):
-            ls.sgemm_batched_strided(int(tb[i]), int(M[i]), int(N[i]), int(K[i]), 1.0,
-                                     dA.data_ptr() + 4 * int(offs[0][i]), 0,
-                                     dB.data_ptr() + 4 * int(offs[1][i]), 0, float(beta[i]),
-                                     dC.data_ptr() + 4 * int(offs[2][i]), 0, 1)
-    ms_pc = _time_events(torch, s, percall, 1, 1)
-    pc = float(2.0 * (M[:sample] * N[:sample] * K[:sample]).sum()) / (ms_pc / 1e3) / 1e9
-    res["per_call_fp32"] = {"gflops": pc, "sample_gemms": sample}
+        def all_shapes():
+            for (M, N, K, A, B, C) in bufs:
+                ls.sgemm_mp(0, 0, C, A, B, M, N, K)
+        ms, reps, clk = _timed_with_clocks(torch, s, all_shapes, args)
+        for (M, N, K, A, B, C) in bufs:
+            msi = _time_events(torch, s, lambda: ls.sgemm_mp(0, 0, C, A, B, M, N, K),
+                               args.steps, args.warmup)
+            per[f"{M}x{N}x{K}"].update(ms=msi, gflops=2.0 * M * N * K / (msi / 1e3) / 1e9)
+        flops = sum(2.0 * M * N * K for (M, N, K) in IRREGULAR)
+        res[name] = {"gflops": flops / (ms / 1e3) / 1e9, "ms_all_shapes": ms,
+                     "timed_passes": reps, "clocks": clk, "shapes": per}
     ls.set_precision(ls.PREC_FP32)
-    best = "bf16x6"
-    _emit("mixed uneven SGEMM batch GFLOP/s (50,000 GEMMs, log-uniform 4..256)",
-          res[best]["gflops"], "GFLOP/s", res[best]["ms"], args,
-          {"workload": "LibShalom_sgemm_batched, M,N,K log-uniform integers in [4,256], "
-                       "NN/NT 50/50, alpha 1, beta 0/1", "gemms": count, "mode": best,
-           "step_gflop": flops / 1e9, "step_gbytes": alg_bytes / 1e9},
-          alg_bytes,
-          {"dtype": "f32 (bf16 split products, f32 accumulate)", "modes": res,
-           "speedup_vs_per_call": res[best]["gflops"] / pc, "gpu_launches": 6 * args.steps})
+    ls.set_splitk(0)
+    ok = {k: v for k, v in res.items()
+          if max(x["max_normwise_err"] for x in v["shapes"].values()) <= 1e-6}
+    best = max(ok, key=lambda k: ok[k]["gflops"])
+    alg_bytes = sum(4.0 * (M * K + K * N + M * N) for (M, N, K) in IRREGULAR)
+    flops = sum(2.0 * M * N * K for (M, N, K) in IRREGULAR)
+    out = {"metric": "irregular SGEMM (sgemm_mp) aggregate GFLOP/s over the six shapes",
+           "value": res[best]["gflops"], "unit": "GFLOP/s", "ms_per_step": res[best]["ms_all_shapes"],
+           "mode": best,
+           "max_normwise_err": max(x["max_normwise_err"] for x in res[best]["shapes"].values()),
+           "config": {"workload": "LibShalom_sgemm_mp NN on (64,3136,576) (128,784,1152) "
+                                  "(256,196,2304) (512,49,4608) (20480,32,20480) (32,20480,4096), "
+                                  "one call per shape per step", "step_gflop": flops / 1e9,
+                      "step_gbytes": alg_bytes / 1e9,
+                      "l2": "2.2 GB of 2.25 GB per step in the 20480 x 32 x 20480 and "
+                            "32 x 20480 x 4096 shapes, which exceed L2"},
+           "roofline": _roofline(alg_bytes, res[best]["ms_all_shapes"], f"sgemm_mp ({best})"),
+           "clocks": res[best]["clocks"], "modes": res,
+           "speedup_vs_reference_order": res[best]["gflops"] / res["fp32_reference_order"]["gflops"]}
+    if cpu:
+        from oracle import oracle as orc
+        threads = orc.max_threads()
+        t = 0.0
+        for (M, N, K, A, B, C) in bufs:
+            hA, hB = A.cpu().numpy(), B.cpu().numpy()
+            t0 = time.perf_counter()
+            orc.port_sgemm_mp(hA, hB, 0, threads)
+            t += time.perf_counter() - t0
+        out["cpu_baseline"] = {"value": flops / t / 1e9, "unit": "GFLOP/s", "cores": threads,
+                               "kind": "port",
+                               "sample": _cpu_desc(f"all six shapes once ({flops / 1e9:.1f} "
+                                                   f"GFLOP in {t:.2f} s), NGM/MGN drivers with "
+                                                   f"the Tm x Tn thread grid", threads)}
+    return out
+
+
+def _print_secondary(args, out):
+    line = {"metric": out.pop("metric"), "value": out.pop("value"), "unit": out.pop("unit"),
+            "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": out.pop("ms_per_step"), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "data": "synthetic", "e2e": None}
+    line.update(out)
+    print(json.dumps(line), flush=True)
+
+
+def wl_irregular(args):
+    torch, ls, s = _gpu_setup()
+    _print_secondary(args, measure_irregular(args, torch, ls, s, cpu=not args.no_cpu))
+
+
+def wl_dgemm_runs(args):
+    torch, ls, s = _gpu_setup()
+    _print_secondary(args, measure_dgemm_runs(args, torch, ls, s, cpu=not args.no_cpu))
+
+
+def wl_mixed(args):
+    torch, ls, s = _gpu_setup()
+    _print_secondary(args, measure_mixed(args, torch, ls, s, cpu=not args.no_cpu))
 
 
 def main():
