@@ -652,6 +652,7 @@ int launch_tc(const LibShalom_dgemm_entry *entries, long count, const DwPlan &pl
 // warp kernel, the others through the CUDA-core tile kernel.  Workspace: two
 // run counts + four arrays sized by the entry count.
 int run_dgemm_warp(const LibShalom_dgemm_entry *entries, long count, int method, int slices) {
+  if (method == LIBSHALOM_DGEMM_DMMA) return run_dgemm_dmma(entries, count);
   State &st = state();
   if (count > (1L << 30)) return LIBSHALOM_ERR_UNSUPPORTED;
   void *ws = nullptr;

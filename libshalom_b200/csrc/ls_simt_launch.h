@@ -38,6 +38,9 @@ int run_dgemm_runs_list(const LibShalom_dgemm_entry *entries, long count, const 
 // ls_dgemm_warp.cu: runs with M, N <= 32 on the FP64 (DMMA) or INT8 (Ozaki)
 // tensor cores, the rest through run_dgemm_runs_list
 int run_dgemm_warp(const LibShalom_dgemm_entry *entries, long count, int method, int slices);
+// ls_dgemm_dmma.cu: runs with M, N <= 32 on the FP64 tensor cores (warp per
+// run, bulk-copy ring), the rest through run_dgemm_runs_list
+int run_dgemm_dmma(const LibShalom_dgemm_entry *entries, long count);
 
 // Plain FP32 split-K GEMM (GEMM_K-aligned slices, rounding order of the mp
 // path per slice) with the partial sums in `partial` (>= splits * M * N

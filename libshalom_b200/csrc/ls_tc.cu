@@ -1220,6 +1220,12 @@ __device__ __forceinline__ bool q_get(const unsigned char *smem, long j, GItem &
   return true;
 }
 
+// C[i] += v at L2 (red.global.add.f32: round to nearest even; subnormal
+// inputs and sums flush to zero)
+__device__ __forceinline__ void red_add_f32(float *p, float v) {
+  asm volatile("red.global.add.f32 [%0], %1;" ::"l"(p), "f"(v) : "memory");
+}
+
 __device__ __forceinline__ void cp_async_mbar_arrive(uint64_t *bar) {
   asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];" ::"r"(ptx::smem_u32(bar))
                : "memory");
@@ -1615,7 +1621,11 @@ __global__ void __launch_bounds__(G_THREADS, 1) k_tc_grouped(const GrpArgs g) {
       const int i0 = c_begin * 8, n_rows = max(0, min(mrows, c_end * 8) - i0);
       const long ld = it.ldc;
       float *c0 = it.C + (long)(it.m0 + i0) * ld + it.n0 + jc;
-      const bool rd = cok && it.beta != 0.0f;
+      // beta == 1 (accumulation, and every run's later products): C += R by
+      // fire-and-forget reductions, so no read of C waits in this warp's
+      // item order; other nonzero betas read C first
+      const bool acc1 = it.beta == 1.0f;
+      const bool rd = cok && it.beta != 0.0f && !acc1;
       float R[32];
 #pragma unroll
       for (int t = 0; t < 32; ++t) R[t] = 0.0f;
@@ -1649,14 +1659,18 @@ __global__ void __launch_bounds__(G_THREADS, 1) k_tc_grouped(const GrpArgs g) {
       __syncwarp();
       if (ok && lane == 0) mbar_arrive(&qempty[j % GQ]);
       if (!ok || !cok) continue;
-      {
+      if (acc1) {
+#pragma unroll
+        for (int t = 0; t < 32; ++t)
+          if (t < n_rows) red_add_f32(c0 + (long)t * ld, R[t]);
+      } else {
         float *pc = c0;
 #pragma unroll
         for (int g8 = 0; g8 < 4; ++g8) {
           float cv[8];
 #pragma unroll
           for (int w = 0; w < 8; ++w)
-            cv[w] = rd && g8 * 8 + w < n_rows ? pc[(long)w * ld] : 0.0f;
+            cv[w] = rd && g8 * 8 + w < n_rows ? __ldcg(pc + (long)w * ld) : 0.0f;  // L2: sees earlier reductions
 #pragma unroll
           for (int w = 0; w < 8; ++w) {
             const int t = g8 * 8 + w;
