@@ -52,14 +52,16 @@ __global__ void k_im2col(const float *x, long c, long h, long w, long kh, long k
 // op(B)[k][p] of the convolution GEMM y[oc][p] = wt[oc][k] col[k][p]: the
 // im2col element for k = (ci, r, q), p = (oy, ox), read from the image
 struct ConvB {
+  static constexpr bool kDense = false;
   const float *x;  // this image, [c][h][w]
   int h, w, kw, khw, sh, sw, ph, pw, ow;
-  __device__ __forceinline__ float operator()(const GemmArgs<float> &, long k, long p) const {
+  // address of the element, nullptr in the zero padding
+  __device__ __forceinline__ const float *ptr(const GemmArgs<float> &, long k, long p) const {
     const int kk = (int)k, pp = (int)p;
     const int ci = kk / khw, rq = kk - ci * khw, r = rq / kw, q = rq - r * kw;
     const int oy = pp / ow, ox = pp - oy * ow;
     const int iy = oy * sh - ph + r, ix = ox * sw - pw + q;
-    return (iy >= 0 && iy < h && ix >= 0 && ix < w) ? x[((long)ci * h + iy) * w + ix] : 0.0f;
+    return (iy >= 0 && iy < h && ix >= 0 && ix < w) ? x + ((long)ci * h + iy) * w + ix : nullptr;
   }
 };
 
@@ -78,13 +80,13 @@ __global__ void __launch_bounds__(Cfg::NTH)
     const int t = (int)(wi - img * per_img);
     ConvB bi = b;
     bi.x = b.x + img * img_stride;
-    simt_tile<float, Cfg, GEMM_K, ConvB>(g, (long)(t / tiles_n) * Cfg::BM,
+    simt_tile<float, Cfg, GEMM_K, false, false, ConvB>(g, (long)(t / tiles_n) * Cfg::BM,
                                     (long)(t % tiles_n) * Cfg::BN, 0, g.K,
                                     g.C + img * g.M * g.N, g.N, 1.0f, 0.0f, smem, bi);
   }
 }
 
-using ConvCfg = SimtCfg<float, 64, 64, 16, 4, 4>;
+using ConvCfg = SimtCfg<float, 64, 64, 4, 4>;
 
 }  // namespace
 

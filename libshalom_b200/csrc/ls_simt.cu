@@ -17,7 +17,7 @@ namespace ls {
 // Single GEMM, persistent over work items (tile_m, tile_n, k-slice).
 // splits == 1: the tile is written to C with alpha/beta.
 // splits > 1: slice z writes its partial to partial[z][M][N].
-template <typename T, class Cfg, int KBLOCK>
+template <typename T, class Cfg, int KBLOCK, bool TA, bool TB>
 __global__ void __launch_bounds__(Cfg::NTH)
 k_gemm_single(GemmArgs<T> g, int tiles_m, int tiles_n, int ways_m, int ways_n,
               int splits, long kchunk, T *partial) {
@@ -51,8 +51,8 @@ k_gemm_single(GemmArgs<T> g, int tiles_m, int tiles_n, int ways_m, int ways_n,
       const long ldo = splits == 1 ? g.ldc : g.N;
       const T alpha = splits == 1 ? g.alpha : T(1);
       const T beta = splits == 1 ? g.beta : T(0);
-      simt_tile<T, Cfg, KBLOCK>(g, (long)tm * Cfg::BM, (long)tn * Cfg::BN, kb, ke, out, ldo,
-                                alpha, beta, smem);
+      simt_tile<T, Cfg, KBLOCK, TA, TB>(g, (long)tm * Cfg::BM, (long)tn * Cfg::BN, kb, ke, out,
+                                        ldo, alpha, beta, smem);
     }
   }
 }
@@ -75,7 +75,7 @@ __global__ void k_splitk_reduce(const T *partial, int splits, long M, long N,
 }
 
 // Uniform batch: work item = (gemm, tile).
-template <typename T, class Cfg>
+template <typename T, class Cfg, bool TB>
 __global__ void __launch_bounds__(Cfg::NTH)
 k_gemm_strided(GemmArgs<T> g, long sA, long sB, long sC, long count,
                int tiles_m, int tiles_n) {
@@ -89,8 +89,8 @@ k_gemm_strided(GemmArgs<T> g, long sA, long sB, long sC, long count,
     h.A = g.A + b * sA;
     h.B = g.B + b * sB;
     h.C = g.C + b * sC;
-    simt_tile<T, Cfg, 0>(h, (t / tiles_n) * Cfg::BM, (t % tiles_n) * Cfg::BN, 0, h.K,
-                         h.C, h.ldc, h.alpha, h.beta, smem);
+    simt_tile<T, Cfg, 0, false, TB>(h, (t / tiles_n) * Cfg::BM, (t % tiles_n) * Cfg::BN, 0, h.K,
+                                    h.C, h.ldc, h.alpha, h.beta, smem);
   }
 }
 
@@ -139,8 +139,14 @@ k_gemm_grouped(const typename EntryOf<T>::type *entries, long count,
         h.ldb = e.ldb > 0 ? e.ldb : (e.transb ? e.K : e.N);
         h.ldc = e.ldc > 0 ? e.ldc : e.N;
         h.alpha = (T)e.alpha; h.beta = (T)e.beta;
-        simt_tile<T, Cfg, 0>(h, (long)(t / tiles_n) * Cfg::BM, (long)(t % tiles_n) * Cfg::BN,
-                             0, h.K, h.C, h.ldc, h.alpha, h.beta, smem);
+        if (h.transb)
+          simt_tile<T, Cfg, 0, false, true>(h, (long)(t / tiles_n) * Cfg::BM,
+                                            (long)(t % tiles_n) * Cfg::BN, 0, h.K, h.C, h.ldc,
+                                            h.alpha, h.beta, smem);
+        else
+          simt_tile<T, Cfg, 0, false, false>(h, (long)(t / tiles_n) * Cfg::BM,
+                                             (long)(t % tiles_n) * Cfg::BN, 0, h.K, h.C, h.ldc,
+                                             h.alpha, h.beta, smem);
       }
     }
   }
@@ -149,35 +155,37 @@ k_gemm_grouped(const typename EntryOf<T>::type *entries, long count,
 // ---------------------------------------------------------------------------
 // tile configurations
 // ---------------------------------------------------------------------------
-using S32 = SimtCfg<float, 32, 32, 32, 2, 2>;
-using S64 = SimtCfg<float, 64, 64, 16, 4, 4>;
-using S128x32 = SimtCfg<float, 128, 32, 16, 4, 4>;
-using S32x128 = SimtCfg<float, 32, 128, 16, 4, 4>;
-using S128x64 = SimtCfg<float, 128, 64, 16, 8, 4>;
-using S64x128 = SimtCfg<float, 64, 128, 16, 4, 8>;
-using S128 = SimtCfg<float, 128, 128, 16, 8, 8>;
+using S32 = SimtCfg<float, 32, 32, 2, 2>;
+using S64 = SimtCfg<float, 64, 64, 4, 4>;
+using S128x32 = SimtCfg<float, 128, 32, 4, 4>;
+using S32x128 = SimtCfg<float, 32, 128, 4, 4>;
+using S128x64 = SimtCfg<float, 128, 64, 8, 4>;
+using S64x128 = SimtCfg<float, 64, 128, 4, 8>;
+using S128 = SimtCfg<float, 128, 128, 8, 8>;
 
-using D32 = SimtCfg<double, 32, 32, 16, 2, 2>;
-using D64 = SimtCfg<double, 64, 64, 16, 4, 4>;
-using D128x32 = SimtCfg<double, 128, 32, 16, 4, 4>;
-using D32x128 = SimtCfg<double, 32, 128, 16, 4, 4>;
+using D32 = SimtCfg<double, 32, 32, 2, 2>;
+using D64 = SimtCfg<double, 64, 64, 4, 4>;
+using D128x32 = SimtCfg<double, 128, 32, 4, 4>;
+using D32x128 = SimtCfg<double, 32, 128, 4, 4>;
 
 struct CfgInfo {
   int bm, bn, eff_pct, per_sm;
 };
+// configuration of calls with transa == Trans (S64 / D64)
+constexpr int TRANSA_CFG = 1;
 
 template <typename T, class Cfg>
 static size_t smem_of() {
   return (size_t)Cfg::SMEM_ELEMS * sizeof(T);
 }
 
-template <typename T, class Cfg, int KBLOCK>
-static int launch_single(const GemmArgs<T> &g, int splits, long kchunk,
-                         T *partial, int ways_m, int ways_n, int per_sm) {
+template <typename T, class Cfg, int KBLOCK, bool TA, bool TB>
+static int launch_single_l(const GemmArgs<T> &g, int splits, long kchunk,
+                           T *partial, int ways_m, int ways_n, int per_sm) {
   const int tiles_m = (int)cdiv(g.M, Cfg::BM), tiles_n = (int)cdiv(g.N, Cfg::BN);
   const long items = (long)tiles_m * tiles_n * splits;
   const size_t smem = smem_of<T, Cfg>();
-  auto kern = k_gemm_single<T, Cfg, KBLOCK>;
+  auto kern = k_gemm_single<T, Cfg, KBLOCK, TA, TB>;
   per_sm = occupancy_of((const void *)kern, Cfg::NTH, smem, per_sm);
   int grid = ways_m > 0 ? grid_for((long)ways_m * ways_n * splits, per_sm)
                        : grid_for(items, per_sm);
@@ -185,6 +193,25 @@ static int launch_single(const GemmArgs<T> &g, int splits, long kchunk,
                                                  splits, kchunk, partial);
   LS_CUDA_TRY(cudaGetLastError());
   return LIBSHALOM_SUCCESS;
+}
+
+// NN and NT layouts for every configuration; A stored K x M (transa) only for
+// TRANSA_CFG, which run_gemm picks for those calls
+template <typename T, class Cfg, int KBLOCK, bool WITH_TA>
+static int launch_single(const GemmArgs<T> &g, int splits, long kchunk,
+                         T *partial, int ways_m, int ways_n, int per_sm) {
+  if constexpr (WITH_TA) {
+    if (g.transa)
+      return g.transb ? launch_single_l<T, Cfg, KBLOCK, true, true>(g, splits, kchunk, partial,
+                                                                     ways_m, ways_n, per_sm)
+                      : launch_single_l<T, Cfg, KBLOCK, true, false>(g, splits, kchunk, partial,
+                                                                      ways_m, ways_n, per_sm);
+  }
+  if (g.transa) return LIBSHALOM_ERR_INVALID_VALUE;
+  return g.transb ? launch_single_l<T, Cfg, KBLOCK, false, true>(g, splits, kchunk, partial,
+                                                                  ways_m, ways_n, per_sm)
+                  : launch_single_l<T, Cfg, KBLOCK, false, false>(g, splits, kchunk, partial,
+                                                                   ways_m, ways_n, per_sm);
 }
 
 // ---------------------------------------------------------------------------
@@ -245,10 +272,10 @@ static int pick_splits(long tiles, long K, int sms, int cap, int forced) {
 template <typename T>
 struct Dispatch;
 
-#define LS_SINGLE_CASE(IDX, CFG)                                               \
-  case IDX:                                                                    \
-    return kblock ? launch_single<T, CFG, 320>(g, splits, kchunk, partial, wm, wn, per_sm) \
-                  : launch_single<T, CFG, 0>(g, splits, kchunk, partial, wm, wn, per_sm);
+#define LS_SINGLE_CASE(IDX, CFG, TA)                                                   \
+  case IDX:                                                                            \
+    return kblock ? launch_single<T, CFG, 320, TA>(g, splits, kchunk, partial, wm, wn, per_sm) \
+                  : launch_single<T, CFG, 0, TA>(g, splits, kchunk, partial, wm, wn, per_sm);
 
 template <>
 struct Dispatch<float> {
@@ -257,13 +284,13 @@ struct Dispatch<float> {
     using T = float;
     const int per_sm = kSCfgs[cfg].per_sm;
     switch (cfg) {
-      LS_SINGLE_CASE(0, S32)
-      LS_SINGLE_CASE(1, S64)
-      LS_SINGLE_CASE(2, S128x32)
-      LS_SINGLE_CASE(3, S32x128)
-      LS_SINGLE_CASE(4, S128x64)
-      LS_SINGLE_CASE(5, S64x128)
-      LS_SINGLE_CASE(6, S128)
+      LS_SINGLE_CASE(0, S32, false)
+      LS_SINGLE_CASE(1, S64, true)
+      LS_SINGLE_CASE(2, S128x32, false)
+      LS_SINGLE_CASE(3, S32x128, false)
+      LS_SINGLE_CASE(4, S128x64, false)
+      LS_SINGLE_CASE(5, S64x128, false)
+      LS_SINGLE_CASE(6, S128, false)
     }
     return LIBSHALOM_ERR_INVALID_VALUE;
   }
@@ -278,10 +305,10 @@ struct Dispatch<double> {
     const int per_sm = kDCfgs[cfg].per_sm;
     (void)kblock;
     switch (cfg) {
-      case 0: return launch_single<T, D32, 0>(g, splits, kchunk, partial, wm, wn, per_sm);
-      case 1: return launch_single<T, D64, 0>(g, splits, kchunk, partial, wm, wn, per_sm);
-      case 2: return launch_single<T, D128x32, 0>(g, splits, kchunk, partial, wm, wn, per_sm);
-      case 3: return launch_single<T, D32x128, 0>(g, splits, kchunk, partial, wm, wn, per_sm);
+      case 0: return launch_single<T, D32, 0, false>(g, splits, kchunk, partial, wm, wn, per_sm);
+      case 1: return launch_single<T, D64, 0, true>(g, splits, kchunk, partial, wm, wn, per_sm);
+      case 2: return launch_single<T, D128x32, 0, false>(g, splits, kchunk, partial, wm, wn, per_sm);
+      case 3: return launch_single<T, D32x128, 0, false>(g, splits, kchunk, partial, wm, wn, per_sm);
     }
     return LIBSHALOM_ERR_INVALID_VALUE;
   }
@@ -296,6 +323,7 @@ int run_gemm(const GemmArgs<T> &g, const SimtOptions &opt, SimtPlan *plan_out) {
   if (opt.force_cfg >= ncfg) return LIBSHALOM_ERR_INVALID_VALUE;
   int cfg = opt.force_cfg >= 0 ? opt.force_cfg
                                : pick_cfg(cfgs, ncfg, g.M, g.N, g.K, st.num_sms, st.thread_cap);
+  if (g.transa) cfg = TRANSA_CFG;  // the one configuration built for A stored K x M
   const long tiles = cdiv(g.M, cfgs[cfg].bm) * cdiv(g.N, cfgs[cfg].bn);
   int splits = opt.allow_split ? pick_splits(tiles, g.K, st.num_sms, st.thread_cap, opt.splits)
                                : 1;
@@ -339,7 +367,8 @@ int run_gemm_splitk_external(const GemmArgs<float> &g, int splits, float *partia
   State &st = state();
   int ncfg;
   const CfgInfo *cfgs = Dispatch<float>::cfgs(&ncfg);
-  const int cfg = pick_cfg(cfgs, ncfg, g.M, g.N, g.K, st.num_sms, st.thread_cap);
+  const int cfg = g.transa ? TRANSA_CFG
+                          : pick_cfg(cfgs, ncfg, g.M, g.N, g.K, st.num_sms, st.thread_cap);
   // K slices stay whole GEMM_K blocks; K = 0 is one empty slice (C = beta C)
   const long kchunk = g.K > 0 ? cdiv(cdiv(g.K, splits), 320) * 320 : 1;
   const int used = g.K > 0 ? (int)cdiv(g.K, kchunk) : 1;
@@ -374,7 +403,7 @@ static int launch_strided(const GemmArgs<T> &g, long sA, long sB, long sC, long 
   const int tiles_m = (int)cdiv(g.M, Cfg::BM), tiles_n = (int)cdiv(g.N, Cfg::BN);
   const long items = (long)tiles_m * tiles_n * count;
   const size_t smem = smem_of<T, Cfg>();
-  auto kern = k_gemm_strided<T, Cfg>;
+  auto kern = g.transb ? k_gemm_strided<T, Cfg, true> : k_gemm_strided<T, Cfg, false>;
   per_sm = occupancy_of((const void *)kern, Cfg::NTH, smem, per_sm);
   const int grid = grid_for(items, per_sm);
   kern<<<grid, Cfg::NTH, smem, state().stream>>>(g, sA, sB, sC, count, tiles_m, tiles_n);
