@@ -333,7 +333,7 @@ class Machine:
             return None
         if op in ("ldr", "str", "ldp", "stp"):
             return self._ldst(op, args)
-        if op in ("ld1", "st1", "st4"):
+        if op in ("ld1", "ld2", "ld3", "ld4", "st1", "st2", "st3", "st4"):
             return self._ldst_struct(op, args)
         return self._integer(op, args)
 
@@ -417,28 +417,54 @@ class Machine:
         return None
 
     def _ldst_struct(self, op, args):
+        """ldN / stN, N = 1..4, on 32- or 64-bit elements: the single-lane form
+        {Vt.s, ...}[lane] moves element `lane` of each register to / from N
+        consecutive elements; the multiple-structure form {Vt.4s, ...}
+        interleaves N registers element by element (N = 1 with several
+        registers: consecutive registers)."""
         m = re.match(r"\{([^}]*)\}(\[(\d)\])?\s*,\s*(.*)$", args)
         regs = [r.strip() for r in m.group(1).split(",")]
         lane = int(m.group(3)) if m.group(3) is not None else None
         a, wb = self.addr(m.group(4))
-        if op == "st4":
-            data = np.array([self.f32(self.vreg(r))[lane] for r in regs], np.float32)
-            self.mem.write(a, data)
-        elif lane is not None:
-            vr = self.vreg(regs[0])
-            if op == "ld1":
-                self.f32(vr)[lane] = self.mem.read(a, 4).view(np.float32)[0]
+        nst = int(op[2])
+        load = op.startswith("ld")
+        arr = re.match(r"v\d+\.(\d*)([sd])", regs[0])
+        esize = 4 if arr.group(2) == "s" else 8
+        dt = np.float32 if esize == 4 else np.float64
+        vr = [self.vreg(r) for r in regs]
+
+        def view(r):
+            return self.v[r].view(dt)
+        if lane is not None:
+            assert len(vr) == nst, args
+            if load:
+                data = self.mem.read(a, esize * nst).view(dt)
+                for i, r in enumerate(vr):
+                    view(r)[lane] = data[i]
             else:
-                self.mem.write(a, self.f32(vr)[lane:lane + 1])
+                self.mem.write(a, np.array([view(r)[lane] for r in vr], dt))
         else:
-            vr = self.vreg(regs[0])
-            assert regs[0].endswith(".2s"), regs
-            if op == "ld1":
-                data = self.mem.read(a, 8)
-                self.v[vr] = 0
-                self.v[vr][:8] = data
+            lanes = int(arr.group(1)) if arr.group(1) else 16 // esize
+            nbytes = esize * lanes * len(vr)
+            if nst == 1:
+                # consecutive registers, no interleave
+                if load:
+                    data = self.mem.read(a, nbytes)
+                    for i, r in enumerate(vr):
+                        self.v[r] = 0
+                        self.v[r][:esize * lanes] = data[i * esize * lanes:(i + 1) * esize * lanes]
+                else:
+                    self.mem.write(a, np.concatenate([self.v[r][:esize * lanes] for r in vr]))
             else:
-                self.mem.write(a, self.v[vr][:8])
+                assert len(vr) == nst, args
+                if load:
+                    data = self.mem.read(a, nbytes).view(dt).reshape(lanes, nst)
+                    for i, r in enumerate(vr):
+                        self.v[r] = 0
+                        view(r)[:lanes] = data[:, i]
+                else:
+                    data = np.stack([view(r)[:lanes] for r in vr], axis=1).astype(dt)
+                    self.mem.write(a, data.reshape(-1).view(np.uint8))
         if wb:
             self.wx(*wb)
         return None
@@ -513,6 +539,36 @@ def run_kernel(path: str, func: str, A: np.ndarray, B: np.ndarray, C: np.ndarray
     if missing:
         raise ValueError(f"unbound asm operands {missing}")
     mach = Machine(prog, labels, params, mem, sp=STACK_TOP)
+    mach.run()
+    if mach.sp != STACK_TOP:
+        raise RuntimeError("stack pointer not restored")
+    return mach.count
+
+
+def run_asm(path: str, func: str, buffers: dict, params: dict, offsets: dict | None = None,
+            stack_bytes: int = 1 << 20, _cache: dict = {}) -> int:
+    """Executes the asm block of `func` with named buffers (numpy arrays,
+    updated in place) and scalar operands.  `offsets` gives, per buffer
+    operand, the element offset its pointer operand starts at.  Returns the
+    number of instructions executed."""
+    key = (path, func)
+    if key not in _cache:
+        lines, names = extract_asm(path, func)
+        _cache[key] = (build_program(lines), names)
+    (prog, labels), names = _cache[key]
+    mem = Memory()
+    p = dict(params)
+    base = 0x10_0000_0000
+    for name, arr in buffers.items():
+        mem.add(base, arr)
+        p[name] = base + (offsets or {}).get(name, 0) * arr.itemsize
+        base += 0x10_0000_0000
+    stack = np.zeros(stack_bytes, np.uint8)
+    mem.add(STACK_TOP - stack_bytes, stack)
+    missing = [n for n in names if n not in p]
+    if missing:
+        raise ValueError(f"unbound asm operands {missing}")
+    mach = Machine(prog, labels, p, mem, sp=STACK_TOP)
     mach.run()
     if mach.sp != STACK_TOP:
         raise RuntimeError("stack pointer not restored")

@@ -44,8 +44,68 @@ def save(name, **kw):
     print("wrote", name, flush=True)
 
 
+def ngm_nn_single_thread(nnlib, A, B, M, N, K):
+    """LibShalom_sgemm_mp's N >> M driver (Small_NGM_NN_SGEMM,
+    NN_LIB/SMM_NN_new.c:92-280) with one thread (T = Tm = Tn = 1), M <= GEMM_M:
+    per GEMM_K = 320 block of K, the reference's own 8 x 12 micro-kernel SMM
+    (NN_LIB/Kernel/SMM_m8n12_new.h:2846) over the N - N % 24 columns and its
+    12 / 8 / 4 / 2 / 1-column edge kernels (SGEBP_NGM_NN, SMM_NN_new.c:8-88)
+    run on the interpreter, with k_tag = the block's first k (0: store, else
+    add into C) and m_tag = 0 (the kernels pack B as they go).  A is packed by
+    NPACK (PACK.c:4) into [k][8 rows] blocks; that pass only moves data and is
+    restated here as the transpose it is."""
+    smm = os.path.join(nnlib, "Kernel", "SMM_m8n12_new.h")
+    GK = 320
+    C = np.full((M, N), np.nan, np.float32)
+    Ac = np.zeros(K * M + 64, np.float32)
+    for kk in range(0, K, GK):
+        kc = min(GK, K - kk)
+        for m0 in range(0, M, 8):
+            mb = min(8, M - m0)
+            Ac[kk * M + m0 * kc:kk * M + m0 * kc + kc * mb] = A[m0:m0 + mb, kk:kk + kc].T.ravel()
+    Bc = np.zeros(N * GK + 64, np.float32)
+    SSB = np.zeros(GK * 24 + 64, np.float32)
+    Bf, Cf = np.ascontiguousarray(B).ravel(), C.ravel()
+    n = 0
+    for kk in range(0, K, GK):
+        kc = min(GK, K - kk)
+        edge = N % 24
+        body = N - edge
+        common = dict(M=M, K=kc, LN=N, LK=K, k_tag=kk, m_tag=0, id_tag=0)
+        bufs = {"C": Cf, "A": Ac, "B": Bf, "Bc": Bc, "SB": SSB}
+        if body:
+            n += emu.run_asm(smm, "SMM", bufs, dict(common, N=body, stride_Bc=kc * 48),
+                             {"A": kk * M, "B": kk * N})
+        off = body
+        for w, fn in ((12, "SMM"), (8, "SMM_NN_KERNEL8x8"), (4, "SMM_NN_KERNEL8x4"),
+                      (2, "SMM_NN_KERNEL8x2"), (1, "SMM_NN_KERNEL8x1")):
+            if edge >= w:
+                extra = dict(stride_Bc=kc * 48) if fn == "SMM" else {}
+                n += emu.run_asm(smm, fn, bufs, dict(common, N=w, **extra),
+                                 {"C": off, "A": kk * M, "B": kk * N + off, "Bc": off * kc})
+                edge -= w
+                off += w
+    return C, n
+
+
 def main(ref_root):
     nnlib = os.path.join(ref_root, "NN_LIB")
+    # LibShalom_sgemm_mp, N >> M (NGM) NN driver with its GEMM_K = 320 blocking
+    # and k_tag accumulation; M a multiple of 8 as in the irregular shapes.
+    # When a K block is not a multiple of 4 and N % 24 >= 12, the reference's
+    # 12-column edge (the N == 12 packing path of SMM jumps past its K % 4
+    # loop) drops the tail terms: edge_cols records those columns.
+    for i, (M, N, K) in enumerate([(16, 96, 700), (8, 100, 333), (24, 60, 960), (32, 75, 1000),
+                                   (16, 45, 500), (8, 39, 650), (40, 22, 333)]):
+        seed = 300 + i
+        A, B = orc.gemm_inputs_f32(seed, M, N, K, 0)
+        C, n = ngm_nn_single_thread(nnlib, A, B, M, N, K)
+        body = N - N % 24
+        tail_blocks = any(min(320, K - kk) % 4 for kk in range(0, K, 320))
+        edge = np.arange(body, body + 12) if (N % 24 >= 12 and tail_blocks) else np.arange(0)
+        save(f"sgemm_mp_ngm_{M}x{N}x{K}_seed{seed}.npz", kind="sgemm_mp_ngm_ref",
+             kernel="Small_NGM_NN_SGEMM (one thread)", M=M, N=N, K=K, seed=seed, C=C,
+             edge_cols=edge, instructions=n)
     # config 1: LibShalom_sgemm(NoTrans, Trans), 80^3, seed 0 -> SGEMM_NT
     # config 2 NT shapes, seeds 16 + n/8
     for n, seed in [(80, 0), (16, 18), (48, 22)]:

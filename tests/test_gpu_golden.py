@@ -2,7 +2,9 @@
 reference's own instructions (tests/golden/make_golden.py executes them on
 oracle/neon_emu.py), through the C ABI.
 
-SGEMM NN (SGEMM_NN_L1 / SGEMM_NN): bit-exact.  SGEMM NT (SGEMM_NT, incl. the
+SGEMM NN (SGEMM_NN_L1 / SGEMM_NN): bit-exact.  LibShalom_sgemm_mp (the
+reference's NGM driver with its GEMM_K = 320 blocks, SMM_NN_new.c:92-280):
+bit-exact outside the reference's defective 12-column edge.  SGEMM NT (SGEMM_NT, incl. the
 80^3 seed-0 call LibShalom_sgemm(NoTrans, Trans)): bit-exact on every row the
 reference computes k-sequentially (rows >= 5 of each strip), and within the
 FP32 bound elsewhere (its first row block uses a lane-split order).  DGEMM
@@ -28,6 +30,22 @@ def test_gpu_matches_reference_fixture(path):
     kind, A, B, Cref = load_fixture(path)
     M, N = Cref.shape
     K = A.shape[1]
+    if kind == "sgemm_mp_ngm_ref":
+        # LibShalom_sgemm_mp without split-K: the GEMM_K = 320 blocked order of
+        # the reference's NGM driver, bit for bit outside its defective edge
+        dC = torch.full((M, N), float("nan"), device="cuda")
+        ls.set_splitk(1)
+        try:
+            ls.sgemm_mp(ls.NoTrans, ls.NoTrans, dC, to_dev(A), to_dev(B), M, N, K)
+        finally:
+            ls.set_splitk(0)
+        C = to_host(dC)
+        ok = np.ones(N, bool)
+        ok[np.load(path)["edge_cols"]] = False
+        assert np.array_equal(C[:, ok], Cref[:, ok])
+        ref = orc.sgemm_f64(A, B, 0)
+        assert componentwise_err(C, ref, orc.sgemm_absprod(A, B, 0)) <= fp32_bound(K)
+        return
     if kind.startswith("sgemm"):
         tb = 1 if kind == "sgemm_nt_ref" else 0
         dC = torch.full((M, N), float("nan"), device="cuda")

@@ -106,3 +106,23 @@ def test_guard_zone_reads_are_nan():
     C = np.zeros(8, np.float32)
     run(["ldr x1, %[A]", "ldr x3, %[C]", "ldr q0, [x1, #16]", "str q0, [x3]"], A=A, C=C)
     assert np.isnan(C[:4]).all()
+
+
+def test_interleaved_structure_loads_and_stores():
+    # ld2 / ld3 de-interleave, st2 interleaves, lane forms move one element per register
+    A = np.arange(24, dtype=np.float32)
+    C = np.zeros(32, np.float32)
+    run(["ldr x1, %[A]", "ldr x2, %[C]",
+         "ld2 {v0.4s, v1.4s}, [x1]",          # v0 = A[0,2,4,6], v1 = A[1,3,5,7]
+         "str q0, [x2]", "str q1, [x2, #16]",
+         "ld3 {v2.4s, v3.4s, v4.4s}, [x1]",   # v2 = A[0,3,6,9], v3 = A[1,4,7,10]
+         "str q2, [x2, #32]", "str q3, [x2, #48]",
+         "st2 {v2.s, v3.s}[1], [x2, #64]",    # A[3], A[4]
+         "ld2 {v5.s, v6.s}[2], [x1, #8]",     # lane 2 of v5 / v6 <- A[2], A[3]
+         "str q5, [x2, #72]", "str q6, [x2, #88]",
+         "st2 {v0.4s, v1.4s}, [x1]"], A=A, C=C)    # interleaves back: A unchanged
+    assert np.array_equal(C[0:4], [0, 2, 4, 6]) and np.array_equal(C[4:8], [1, 3, 5, 7])
+    assert np.array_equal(C[8:12], [0, 3, 6, 9]) and np.array_equal(C[12:16], [1, 4, 7, 10])
+    assert np.array_equal(C[16:18], [3, 4])
+    assert C[18 + 2] == 2.0 and C[22 + 2] == 3.0
+    assert np.array_equal(A, np.arange(24, dtype=np.float32))
