@@ -136,7 +136,8 @@ LIBSHALOM_API int LibShalom_set_splitk(int splits);
  * (0..6 FP32: 32x32, 64x64, 128x32, 32x128, 128x64, 64x128, 128x128;
  * 0..3 FP64: 32x32, 64x64, 128x32, 32x128; -1 = table/model); a value the
  * data type does not have makes the call fail with
- * LIBSHALOM_ERR_INVALID_VALUE.  set_autotune(0) ignores the table.
+ * LIBSHALOM_ERR_INVALID_VALUE; calls with transa == Trans always use
+ * configuration 1 (64x64).  set_autotune(0) ignores the table.
  * get_plan reports the tile configuration (-1 on the tensor-core path) and
  * split-K factor of the last single / mp call and the table's entry count. */
 LIBSHALOM_API int LibShalom_set_tile_config(int cfg);
