@@ -97,7 +97,7 @@ int occupancy_of(const void *kern, int threads, size_t smem, int fallback) {
   std::lock_guard<std::mutex> lk(m);
   auto it = cache.find(kern);
   if (it != cache.end()) return it->second;
-  if (smem > 48 * 1024 &&
+  if (smem >= 48 * 1024 &&
       cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
           cudaSuccess) {
     cudaGetLastError();

@@ -25,3 +25,29 @@ def pytest_collection_modifyitems(config, items):
     for it in items:
         if "gpu" in it.keywords:
             it.add_marker(skip)
+
+
+@pytest.fixture(autouse=True)
+def _library_defaults(request):
+    """After every GPU test, the library's process-wide settings go back to
+    their defaults (whatever the test did or failed to undo), so that one
+    failing test cannot change the conditions of the next."""
+    yield
+    if "gpu" not in request.keywords:
+        return
+    try:
+        import libshalom_b200 as ls
+        L = ls.lib()
+    except Exception:
+        return
+    L.LibShalom_defer_flush()
+    L.LibShalom_set_sync(1)
+    L.LibShalom_set_stream(None)
+    L.LibShalom_set_precision(0)
+    L.LibShalom_set_dgemm_method(0, 0)
+    L.LibShalom_set_splitk(0)
+    L.LibShalom_set_tile_config(-1)
+    L.LibShalom_set_autotune(1)
+    L.LibShalom_set_graph_cache(0)
+    L.LibShalom_set_thread_nums(0)
+    L.LibShalom_set_tma(1)
