@@ -40,8 +40,9 @@ SIZES = list(range(8, 129, 8))
 LAYOUTS = (0, 1)  # NoTrans (NN), Trans (NT)
 BATCH = 10_000
 METRIC = "batched small-GEMM GFLOP/s (cube sweep 8..128, NN+NT, 10,000 per size)"
-# DRAM bytes per algorithmic byte of the bf16x6 batched kernel, from one ncu
-# capture (profiles/k_tc_ws_bf16x6_nn128_batch2000.md)
+# DRAM bytes per algorithmic byte of the bf16x6 batched kernel: ncu
+# dram__bytes_read.sum + dram__bytes_write.sum of one launch over 2,000 NN
+# GEMMs at n = 128 read 0.910 of the launch's algorithmic bytes
 TRAFFIC_PER_ALG_BYTE = 0.910
 
 
@@ -438,10 +439,9 @@ def run_gpu(args):
         "modes": {names[m]: r for m, r in results.items()},
         "roofline": {"bound": "hbm", "achieved": achieved_gbs, "peak": hbm_peak,
                      "unit": "GB/s", "frac": achieved_gbs / hbm_peak,
-                     # DRAM bytes per launch: ncu dram__bytes_read + write of the same
-                     # kernel on a 2000-GEMM n=128 capture (0.910 per algorithmic byte,
-                     # profiles/k_tc_ws_bf16x6_nn128_batch2000.md), scaled to the
-                     # average launch of this sweep
+                     # DRAM bytes per launch: the measured 0.910 DRAM bytes per
+                     # algorithmic byte of this kernel, scaled to the average
+                     # launch of this sweep
                      "traffic": (TRAFFIC_PER_ALG_BYTE * step_bytes() / n_calls
                                  if best == ls.PREC_BF16X6 else None),
                      "traffic_unit": "bytes per launch",
