@@ -615,6 +615,15 @@ struct WsArgs {
 __device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
   asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(ptx::smem_u32(bar)) : "memory");
 }
+// Arrival that publishes no memory: the default (release) arrive first waits
+// for this thread's earlier global stores to be acknowledged, which costs an
+// epilogue thousands of cycles per tile.  For arrivals that only say "done
+// reading" (TMEM read back and waited for, a queue slot copied into
+// registers) nothing has to be published.
+__device__ __forceinline__ void mbar_arrive_relaxed(uint64_t *bar) {
+  asm volatile("mbarrier.arrive.relaxed.cta.shared::cta.b64 _, [%0];" ::"r"(ptx::smem_u32(bar))
+               : "memory");
+}
 __device__ __forceinline__ void mbar_arrive_tx(uint64_t *bar, uint32_t bytes) {
   asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%1], %0;" ::"r"(bytes),
                "r"(ptx::smem_u32(bar))
@@ -629,18 +638,33 @@ __device__ __forceinline__ void tma_load_3d(uint32_t dst, const CUtensorMap *map
       : "memory");
 }
 
-// Bounded wait that also gives up as soon as another role has aborted.
-// `limit` polls (about a second with the default) before it gives up.
-__device__ __forceinline__ bool ws_wait(uint64_t *bar, uint32_t parity, volatile int *abort_flag,
-                                        unsigned *err, uint32_t limit = 1u << 22) {
+// Slow path of ws_wait: the thread suspends in the barrier wait (up to about
+// a microsecond per try, woken when the phase completes) instead of polling,
+// so waiting roles take no issue slots or shared-memory bandwidth from the
+// working ones.  Gives up after `limit` tries or two seconds, whichever
+// comes first, or as soon as another role has aborted.  Not inlined: every
+// wait of every role shares this one copy of the code.
+__device__ __noinline__ bool ws_wait_slow(uint64_t *bar, uint32_t parity,
+                                          volatile int *abort_flag, unsigned *err,
+                                          uint32_t limit) {
+  const uint64_t t0 = ptx::globaltimer_ns();
   for (uint32_t it = 0; it < limit; ++it) {
-    if (ptx::mbar_try_wait(bar, parity)) return true;
-    if ((it & 255) == 255 && *abort_flag) return false;
-    if (it > 64) __nanosleep(it < 4096 ? 32 : 256);
+    if (ptx::mbar_try_wait_suspend(bar, parity, 1000)) return true;
+    if ((it & 15) == 15) {
+      if (*abort_flag) return false;
+      if (ptx::globaltimer_ns() - t0 > 2000000000ull) break;
+    }
   }
   *abort_flag = 1;
   atomicOr(err, 1u);
   return false;
+}
+
+// Bounded wait: one test inline, the rest in ws_wait_slow.
+__device__ __forceinline__ bool ws_wait(uint64_t *bar, uint32_t parity, volatile int *abort_flag,
+                                        unsigned *err, uint32_t limit = 1u << 22) {
+  if (ptx::mbar_try_wait(bar, parity)) return true;
+  return ws_wait_slow(bar, parity, abort_flag, err, limit);
 }
 
 template <int NSPLIT, bool DRAIN, bool WIDE>
@@ -956,7 +980,7 @@ __global__ void __launch_bounds__(WsRoles<WIDE>::THREADS, 1)
       auto release = [&](int a) {
         ptx::tc_fence_before();
         __syncwarp();
-        if (lane == 0) mbar_arrive(&bars[B_AEMPTY + a]);
+        if (lane == 0) mbar_arrive_relaxed(&bars[B_AEMPTY + a]);
       };
       const bool rows_in = ti.m0 + wq * 32 < p.M;  // G == 1 when ctma
       // chunks holding columns of the GEMMs whose rows this warp covers
@@ -1207,7 +1231,8 @@ __device__ __forceinline__ bool q_get(const unsigned char *smem, long j, GItem &
                                       volatile int *s_abort, unsigned *err) {
   uint64_t *qfull = reinterpret_cast<uint64_t *>(const_cast<unsigned char *>(smem) + G_OFF_QBAR);
   const int slot = (int)(j % GQ);
-  if (!ws_wait(&qfull[slot], (uint32_t)((j / GQ) & 1), s_abort, err)) return false;
+  if (!__all_sync(0xffffffffu, ws_wait(&qfull[slot], (uint32_t)((j / GQ) & 1), s_abort, err)))
+    return false;
   const GSlot s = reinterpret_cast<const GSlot *>(smem + G_OFF_Q)[slot];
   it.A = s.A; it.B = s.B; it.C = s.C;
   it.M = s.M; it.N = s.N; it.K = s.K; it.lda = s.lda;
@@ -1385,33 +1410,39 @@ __global__ void __launch_bounds__(G_THREADS, 1) k_tc_grouped(const GrpArgs g) {
     }
   } else if (warp == G_W_MMA) {
     // -------------------------------- MMA ---------------------------------
-    if (lane == 0) {
-      long js = 0, u = 0;
-      bool ok = true;
-      for (long j = 0; ok; ++j) {
-        GItem it;
-        if (!q_get(smem, j, it, s_abort, g.err)) break;
-        if (it.M < 0) break;
-        // C^T = op(B)^T A^T: the 128 MMA rows (TMEM lanes) are the tile's
-        // columns, the MMA N its rows (rounded to 16)
-        const int mrows = min(TC_BM, it.M - it.m0);
-        const uint32_t idesc = ptx::idesc_bf16_f32(TC_BM, (mrows + 15) / 16 * 16);
-        for (int s = 0; s < it.nk; ++s, ++js) {
-          const int s_in = s % kc;
-          if (s_in == 0) {
-            const int a = (int)(u & 1);
-            if (u >= 2 && !ws_wait(&bars[B_AEMPTY + a], (uint32_t)(((u >> 1) - 1) & 1), s_abort,
-                                   g.err)) {
-              ok = false;
-              break;
-            }
-          }
-          const int b = (int)(js & 1);
-          if (!ws_wait(&bars[B_BFULL + b], (uint32_t)((js >> 1) & 1), s_abort, g.err)) {
+    // The whole warp walks the items and waits, so that none of its lanes
+    // sits at the block barrier while the issuing lane works; lane 0 issues
+    // the MMAs and the commits.
+    const unsigned FULL = 0xffffffffu;
+    long js = 0, u = 0;
+    bool ok = true;
+    for (long j = 0; ok; ++j) {
+      GItem it;
+      if (!q_get(smem, j, it, s_abort, g.err)) break;
+      if (it.M < 0) break;
+      // C^T = op(B)^T A^T: the 128 MMA rows (TMEM lanes) are the tile's
+      // columns, the MMA N its rows (rounded to 16)
+      const int mrows = min(TC_BM, it.M - it.m0);
+      const uint32_t idesc = ptx::idesc_bf16_f32(TC_BM, (mrows + 15) / 16 * 16);
+      for (int s = 0; s < it.nk; ++s, ++js) {
+        const int s_in = s % kc;
+        if (s_in == 0 && u >= 2) {
+          const int a = (int)(u & 1);
+          if (!__all_sync(FULL, ws_wait(&bars[B_AEMPTY + a], (uint32_t)(((u >> 1) - 1) & 1),
+                                        s_abort, g.err))) {
             ok = false;
             break;
           }
-          ptx::tc_fence_after();
+        }
+        const int b = (int)(js & 1);
+        if (!__all_sync(FULL, ws_wait(&bars[B_BFULL + b], (uint32_t)((js >> 1) & 1), s_abort,
+                                      g.err))) {
+          ok = false;
+          break;
+        }
+        ptx::tc_fence_after();
+        const bool last = s_in == kc - 1 || s == it.nk - 1;
+        if (lane == 0) {
           const uint32_t acc_base = tmem + (uint32_t)((u & 1) * 256);
           const uint32_t bb = smem_base + WS_OFF_BUF + b * BUF_BYTES;
           const int ksteps = max(1, min(2, (it.K - s * TC_BK + 15) / 16));
@@ -1436,15 +1467,15 @@ __global__ void __launch_bounds__(G_THREADS, 1) k_tc_grouped(const GrpArgs g) {
             }
           }
           ptx::mma_commit(&bars[B_BEMPTY + b]);
-          if (s_in == kc - 1 || s == it.nk - 1) {
-            ptx::mma_commit(&bars[B_AFULL + (u & 1)]);
-            ++u;
-          }
+          if (last) ptx::mma_commit(&bars[B_AFULL + (u & 1)]);
         }
+        __syncwarp();
+        if (last) ++u;
       }
-      ptx::mma_commit(&bars[B_FINAL]);
-      ptx::mbar_wait_bounded(&bars[B_FINAL], 0);
     }
+    if (lane == 0) ptx::mma_commit(&bars[B_FINAL]);
+    __syncwarp();
+    ptx::mbar_wait_bounded(&bars[B_FINAL], 0);
   } else if (warp < G_W_EPI0) {
     // --------------------- converters (and operand loads) ---------------------
     // The 256 converter threads also stage the operands: before converting
@@ -1474,7 +1505,8 @@ __global__ void __launch_bounds__(G_THREADS, 1) k_tc_grouped(const GrpArgs g) {
       }
       const int st = (int)(jsl % G_STAGES);
       if (jsl >= G_STAGES &&
-          !ws_wait(&bars[B_EMPTY + st], (uint32_t)(((jsl / G_STAGES) - 1) & 1), s_abort, g.err))
+          !__all_sync(0xffffffffu, ws_wait(&bars[B_EMPTY + st],
+                                           (uint32_t)(((jsl / G_STAGES) - 1) & 1), s_abort, g.err)))
         return false;
       const int mrows = min(TC_BM, il.M - il.m0), ncols = min(il.tn, il.N - il.n0);
       const int va = row_vec(il.A, il.lda), vb = row_vec(il.B, il.ldb);
@@ -1528,12 +1560,14 @@ __global__ void __launch_bounds__(G_THREADS, 1) k_tc_grouped(const GrpArgs g) {
           break;
         }
         const int st = (int)(js % G_STAGES), b = (int)(js & 1);
-        if (!ws_wait(&bars[B_FULL + st], (uint32_t)((js / G_STAGES) & 1), s_abort, g.err)) {
+        if (!__all_sync(0xffffffffu, ws_wait(&bars[B_FULL + st], (uint32_t)((js / G_STAGES) & 1),
+                                             s_abort, g.err))) {
           ok = false;
           break;
         }
-        if (js >= 2 && !ws_wait(&bars[B_BEMPTY + b], (uint32_t)(((js >> 1) - 1) & 1), s_abort,
-                                g.err)) {
+        if (js >= 2 && !__all_sync(0xffffffffu, ws_wait(&bars[B_BEMPTY + b],
+                                                        (uint32_t)(((js >> 1) - 1) & 1), s_abort,
+                                                        g.err))) {
           ok = false;
           break;
         }
@@ -1632,7 +1666,8 @@ __global__ void __launch_bounds__(G_THREADS, 1) k_tc_grouped(const GrpArgs g) {
       const int nchunks = (it.nk + kc - 1) / kc;
       for (int cu = 0; cu < nchunks; ++cu, ++u) {
         const int a = (int)(u & 1);
-        if (!ws_wait(&bars[B_AFULL + a], (uint32_t)((u >> 1) & 1), s_abort, g.err)) {
+        if (!__all_sync(0xffffffffu,
+                        ws_wait(&bars[B_AFULL + a], (uint32_t)((u >> 1) & 1), s_abort, g.err))) {
           ok = false;
           break;
         }
@@ -1654,15 +1689,19 @@ __global__ void __launch_bounds__(G_THREADS, 1) k_tc_grouped(const GrpArgs g) {
         }
         ptx::tc_fence_before();
         __syncwarp();
-        if (lane == 0) mbar_arrive(&bars[B_AEMPTY + a]);
+        if (lane == 0) mbar_arrive_relaxed(&bars[B_AEMPTY + a]);
       }
       __syncwarp();
-      if (ok && lane == 0) mbar_arrive(&qempty[j % GQ]);
-      if (!ok || !cok) continue;
+      if (ok && lane == 0) mbar_arrive_relaxed(&qempty[j % GQ]);
+      // the whole warp stays together (lanes past N store nothing): a lane
+      // that ran ahead into the next item would leave the warp diverged at
+      // its collective TMEM loads
+      if (!ok) continue;
+      const int nr = cok ? n_rows : 0;
       if (acc1) {
 #pragma unroll
         for (int t = 0; t < 32; ++t)
-          if (t < n_rows) red_add_f32(c0 + (long)t * ld, R[t]);
+          if (t < nr) red_add_f32(c0 + (long)t * ld, R[t]);
       } else {
         float *pc = c0;
 #pragma unroll
@@ -1670,11 +1709,11 @@ __global__ void __launch_bounds__(G_THREADS, 1) k_tc_grouped(const GrpArgs g) {
           float cv[8];
 #pragma unroll
           for (int w = 0; w < 8; ++w)
-            cv[w] = rd && g8 * 8 + w < n_rows ? __ldcg(pc + (long)w * ld) : 0.0f;  // L2: sees earlier reductions
+            cv[w] = rd && g8 * 8 + w < nr ? __ldcg(pc + (long)w * ld) : 0.0f;  // L2: sees earlier reductions
 #pragma unroll
           for (int w = 0; w < 8; ++w) {
             const int t = g8 * 8 + w;
-            if (t < n_rows) pc[(long)w * ld] = rd ? __fmaf_rn(it.beta, cv[w], R[t]) : R[t];
+            if (t < nr) pc[(long)w * ld] = rd ? __fmaf_rn(it.beta, cv[w], R[t]) : R[t];
           }
           pc += 8 * ld;
         }
