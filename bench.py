@@ -72,6 +72,8 @@ def parse():
     p.add_argument("--sizes", default=None, help="comma list of cube sizes (default 8..128)")
     p.add_argument("--batch", type=int, default=None, help="GEMMs per size (default 10000)")
     p.add_argument("--layouts", default=None, help="nn, nt or nn,nt (default both)")
+    p.add_argument("--count", type=int, default=None,
+                   help="GEMMs of the mixed / dgemm-runs workload (default 50,000 / 200,000)")
     return p.parse_args()
 
 
@@ -711,7 +713,7 @@ def measure_mixed(args, torch, ls, s, count=50_000, cpu=True):
                 "how": "LibShalom_sgemm_batched_strided (plain FP32) once per GEMM, the "
                        "calls captured in one CUDA graph and replayed"}
     best = "bf16x6"
-    out = {"metric": "mixed uneven SGEMM batch GFLOP/s (50,000 GEMMs, log-uniform 4..256)",
+    out = {"metric": f"mixed uneven SGEMM batch GFLOP/s ({count:,} GEMMs, log-uniform 4..256)",
            "value": modes[best]["gflops"], "unit": "GFLOP/s", "ms_per_step": modes[best]["ms"],
            "mode": best, "max_normwise_err": modes[best]["max_normwise_err"],
            "config": {"workload": "LibShalom_sgemm_batched, M,N,K log-uniform integers in "
@@ -836,7 +838,7 @@ def measure_dgemm_runs(args, torch, ls, s, count=200_000, run=8, cpu=True):
                 "how": "LibShalom_dgemm (plain FP64, overwrite semantics) once per product, "
                        "the calls captured in one CUDA graph and replayed"}
     value = methods[best]["gflops"]
-    out = {"metric": "batched uneven DGEMM GFLOP/s (200,000 products, runs of 8 share C)",
+    out = {"metric": f"batched uneven DGEMM GFLOP/s ({count:,} products, runs of {run} share C)",
            "value": value, "unit": "GFLOP/s", "ms_per_step": methods[best]["ms"],
            "method": best, "max_normwise_err": methods[best]["max_normwise_err"],
            "config": {"workload": "LibShalom_dgemm_batched, C += A B, M,N per run and K per "
@@ -963,12 +965,14 @@ def wl_irregular(args):
 
 def wl_dgemm_runs(args):
     torch, ls, s = _gpu_setup()
-    _print_secondary(args, measure_dgemm_runs(args, torch, ls, s, cpu=not args.no_cpu))
+    kw = {"count": args.count} if args.count else {}
+    _print_secondary(args, measure_dgemm_runs(args, torch, ls, s, cpu=not args.no_cpu, **kw))
 
 
 def wl_mixed(args):
     torch, ls, s = _gpu_setup()
-    _print_secondary(args, measure_mixed(args, torch, ls, s, cpu=not args.no_cpu))
+    kw = {"count": args.count} if args.count else {}
+    _print_secondary(args, measure_mixed(args, torch, ls, s, cpu=not args.no_cpu, **kw))
 
 
 def main():

@@ -642,9 +642,10 @@ __device__ __forceinline__ void tma_load_3d(uint32_t dst, const CUtensorMap *map
 // a microsecond per try, woken when the phase completes) instead of polling,
 // so waiting roles take no issue slots or shared-memory bandwidth from the
 // working ones.  Gives up after `limit` tries or two seconds, whichever
-// comes first, or as soon as another role has aborted.  Not inlined: every
-// wait of every role shares this one copy of the code.
-__device__ __noinline__ bool ws_wait_slow(uint64_t *bar, uint32_t parity,
+// comes first, or as soon as another role has aborted.  Inlined: a call
+// would make the caller save its live registers to local memory around every
+// wait.
+__device__ __forceinline__ bool ws_wait_slow(uint64_t *bar, uint32_t parity,
                                           volatile int *abort_flag, unsigned *err,
                                           uint32_t limit) {
   const uint64_t t0 = ptx::globaltimer_ns();
