@@ -40,18 +40,32 @@ SIZES = list(range(8, 129, 8))
 LAYOUTS = (0, 1)  # NoTrans (NN), Trans (NT)
 BATCH = 10_000
 METRIC = "batched small-GEMM GFLOP/s (cube sweep 8..128, NN+NT, 10,000 per size)"
-# DRAM bytes per algorithmic byte of the bf16x6 batched kernel: ncu
-# dram__bytes_read.sum + dram__bytes_write.sum of one launch over 2,000 NN
-# GEMMs at n = 128 read 0.910 of the launch's algorithmic bytes
-TRAFFIC_PER_ALG_BYTE = 0.910
+# DRAM bytes per algorithmic byte of each bf16x6 batched launch of the sweep,
+# by n (mean of NN and NT): ncu dram__bytes_read.sum + dram__bytes_write.sum
+# of one cold launch per size and layout over 2,000 GEMMs.  A and B are read
+# exactly once (0.667 of the algorithmic bytes); C lines still dirty in L2
+# when the launch ends are written back later and are not counted, which is
+# all of C for the packed n <= 64 launches at that batch.
+TRAFFIC_PER_ALG_BYTE = {8: 0.701, 16: 0.675, 24: 0.670, 32: 0.669, 40: 0.668, 48: 0.668,
+                        56: 0.668, 64: 0.668, 72: 0.745, 80: 0.787, 88: 0.818, 96: 0.834,
+                        104: 0.864, 112: 0.878, 120: 0.892, 128: 0.903}
 
 
-def step_flops(batch=BATCH):
+def step_flops(batch=None):
+    batch = BATCH if batch is None else batch
     return sum(2.0 * n ** 3 * batch for n in SIZES for _ in LAYOUTS)
 
 
-def step_bytes(batch=BATCH):
+def step_bytes(batch=None):
+    batch = BATCH if batch is None else batch
     return sum(4.0 * 3 * n * n * batch for n in SIZES for _ in LAYOUTS)
+
+
+def step_traffic(batch=None):
+    """DRAM bytes of one step's launches by the measured per-size ratios."""
+    batch = BATCH if batch is None else batch
+    return sum(TRAFFIC_PER_ALG_BYTE.get(n, 0.903) * 4.0 * 3 * n * n * batch
+               for n in SIZES for _ in LAYOUTS)
 
 
 def parse():
@@ -432,20 +446,20 @@ def run_gpu(args):
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32" if best == ls.PREC_FP32 else "f32 (bf16 split products, f32 accumulate)",
         "data": "synthetic",
-        "config": {"workload": "cube sweep M=N=K in 8..128 step 8, NN and NT, uniform batches "
-                               "of 10,000 FP32 GEMMs per size (32 batched calls per step)",
+        "config": {"workload": f"cube sweep M=N=K in {SIZES[0]}..{SIZES[-1]}, "
+                               f"{'NN and NT' if len(LAYOUTS) == 2 else ('NN' if LAYOUTS[0] == 0 else 'NT')}, "
+                               f"uniform batches of {BATCH:,} FP32 GEMMs per size "
+                               f"({len(SIZES) * len(LAYOUTS)} batched calls per step)",
                    "batch_per_size": BATCH, "step_gflop": step_flops() / 1e9,
                    "step_gbytes": step_bytes() / 1e9, "mode": names[best],
-                   "l2": "inputs larger than L2: 23 GB touched per step",
+                   "l2": f"inputs larger than L2: {step_bytes() / 1e9:.0f} GB touched per step",
                    "parallelism": f"replicas x{world}"},
         "modes": {names[m]: r for m, r in results.items()},
         "roofline": {"bound": "hbm", "achieved": achieved_gbs, "peak": hbm_peak,
                      "unit": "GB/s", "frac": achieved_gbs / hbm_peak,
-                     # DRAM bytes per launch: the measured 0.910 DRAM bytes per
-                     # algorithmic byte of this kernel, scaled to the average
-                     # launch of this sweep
-                     "traffic": (TRAFFIC_PER_ALG_BYTE * step_bytes() / n_calls
-                                 if best == ls.PREC_BF16X6 else None),
+                     # DRAM bytes per launch: the measured per-size ratios
+                     # (TRAFFIC_PER_ALG_BYTE) over the step's launches, averaged
+                     "traffic": (step_traffic() / n_calls if best == ls.PREC_BF16X6 else None),
                      "traffic_unit": "bytes per launch",
                      "peak_source": peak_src,
                      "kernel": "sgemm batched (" + names[best] + ")",
