@@ -802,6 +802,10 @@ __global__ void __launch_bounds__(WsRoles<WIDE>::THREADS, 1)
     const int ct = tid - W_CONV0 * 32;
     const bool nn = !p.transb;
     const int nn_w = args.nn_w;
+    // quotients by tn and N through float reciprocals: exact for the ranges
+    // here (e < 4 tn <= 512, jj < 128), whose fractions stay at least 1/256
+    // away from the next integer
+    const float inv_tn = 1.0f / (float)tn, inv_n = 1.0f / (float)max(1, p.N);
     long j = 0;
     bool ok = true;
     for (long t = blockIdx.x; ok && t < p.num_tiles; t += gridDim.x) {
@@ -844,7 +848,7 @@ __global__ void __launch_bounds__(WsRoles<WIDE>::THREADS, 1)
 #pragma unroll
         for (int q = 0; q < PER; ++q) {
           const int e = ct + q * NCT;
-          const int jj = e % tn, c = e / tn;
+          const int c = (int)(((float)e + 0.5f) * inv_tn), jj = e - c * tn;
           if (e < 4 * tn && jj < b_cols && c < nchunk) {
             float x[8];
             if (!nn) {
@@ -860,7 +864,7 @@ __global__ void __launch_bounds__(WsRoles<WIDE>::THREADS, 1)
               const float *fb = reinterpret_cast<const float *>(stg + 16384);
               int col = jj, gofs = 0;
               if (p.G > 1) {
-                const int g = jj / p.N;
+                const int g = (int)(((float)jj + 0.5f) * inv_n);
                 col = jj - g * p.N;
                 gofs = g * 32 * nn_w;
               }
