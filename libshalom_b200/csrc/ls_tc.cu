@@ -1536,8 +1536,9 @@ __global__ void __launch_bounds__(G_THREADS, 1) k_tc_grouped(const GrpArgs g) {
       } else {
         // [32 k][tn] floats; the valid columns of every k row (zero past K)
         const int cpr = (ncols + 3) >> 2;
+        const float inv_cpr = 1.0f / (float)cpr;  // exact quotients: e < 32 cpr <= 1024
         for (int e = ct; e < 32 * cpr; e += NP) {
-          const int kr = e / cpr, col = (e - kr * cpr) * 4;
+          const int kr = (int)(((float)e + 0.5f) * inv_cpr), col = (e - kr * cpr) * 4;
           const uint32_t dst = sb + (kr * il.tn + col) * 4;
           const float *src = il.B + (long)(k0 + kr) * il.ldb + il.n0 + col;
           stage_chunk(dst, src, kr < kv ? min(4, ncols - col) : 0, vb, il.B);
@@ -1559,6 +1560,8 @@ __global__ void __launch_bounds__(G_THREADS, 1) k_tc_grouped(const GrpArgs g) {
       if (it.M < 0) break;
       const int tn = it.tn;
       const int mrows = min(TC_BM, it.M - it.m0), ncols = min(tn, it.N - it.n0);
+      // e / tn through an exact float reciprocal (e < 4 tn <= 512)
+      const float inv_tn = 1.0f / (float)tn;
       for (int s = 0; s < it.nk; ++s, ++js) {
         if (!issue_next()) {
           ok = false;
@@ -1602,7 +1605,7 @@ __global__ void __launch_bounds__(G_THREADS, 1) k_tc_grouped(const GrpArgs g) {
 #pragma unroll
         for (int q = 0; q < 2; ++q) {
           const int e = ct + q * 256;
-          const int jj = e % tn, c = e / tn;
+          const int c = (int)(((float)e + 0.5f) * inv_tn), jj = e - c * tn;
           if (e < 4 * tn && jj < ncols && c < nchunk) {
             float x[8];
             if (it.transb) {
