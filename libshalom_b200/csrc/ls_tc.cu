@@ -668,7 +668,10 @@ __device__ __forceinline__ bool ws_wait(uint64_t *bar, uint32_t parity, volatile
   return ws_wait_slow(bar, parity, abort_flag, err, limit);
 }
 
-template <int NSPLIT, bool DRAIN, bool WIDE>
+// BLX > 0: each epilogue warp holds at most BLX 32-column blocks of C (a
+// DRAIN kernel for tiles of at most 32 * BLX * (epilogue warps / 4) columns
+// keeps a smaller register fold)
+template <int NSPLIT, bool DRAIN, bool WIDE, int BLX = 0>
 __global__ void __launch_bounds__(WsRoles<WIDE>::THREADS, 1)
     k_tc_ws(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
             const __grid_constant__ CUtensorMap tmC, const WsArgs args) {
@@ -892,7 +895,7 @@ __global__ void __launch_bounds__(WsRoles<WIDE>::THREADS, 1)
     // warp (TMEM lane quarter wq, column group grp) owns the 32-column blocks
     // grp, grp + NG, ... of its 32 rows: chunk q (8 columns) of the warp is
     // tile chunk chunk_of(q)
-    constexpr int NG = Roles::NE / 4, BL = Roles::BLOCKS;
+    constexpr int NG = Roles::NE / 4, BL = BLX > 0 ? BLX : Roles::BLOCKS;
     constexpr int NBUF = 8 / Roles::NE;  // 4 KB staging buffers per warp
     const int ew = warp - Roles::W_EPI;
     const int wq = warp & 3, grp = ew >> 2;
@@ -1862,14 +1865,19 @@ int tc_launch(TcProblem &p, int mode) {
   WsArgs wa;
   if (st.use_tma && ws_maps(p, &ma, &mb, &mc, &wa)) {
     const bool wide = !drain && wa.c_tma;
+    // long K on tiles of at most 64 columns: one 32-column block per epilogue
+    // warp, a fold of 32 registers instead of 64 (no spills)
+    const bool narrow = drain && p.tile_n <= 32 * (WsRoles<false>::NE / 4);
     const void *kern =
         mode == LIBSHALOM_PREC_BF16X6
-            ? (drain  ? (const void *)k_tc_ws<3, true, false>
-               : wide ? (const void *)k_tc_ws<3, false, true>
-                      : (const void *)k_tc_ws<3, false, false>)
-            : (drain  ? (const void *)k_tc_ws<2, true, false>
-               : wide ? (const void *)k_tc_ws<2, false, true>
-                      : (const void *)k_tc_ws<2, false, false>);
+            ? (narrow ? (const void *)k_tc_ws<3, true, false, 1>
+               : drain ? (const void *)k_tc_ws<3, true, false>
+               : wide  ? (const void *)k_tc_ws<3, false, true>
+                       : (const void *)k_tc_ws<3, false, false>)
+            : (narrow ? (const void *)k_tc_ws<2, true, false, 1>
+               : drain ? (const void *)k_tc_ws<2, true, false>
+               : wide  ? (const void *)k_tc_ws<2, false, true>
+                       : (const void *)k_tc_ws<2, false, false>);
     const int threads = wide ? WsRoles<true>::THREADS : WsRoles<false>::THREADS;
     (void)occupancy_of(kern, threads, WS_SMEM, 1);  // raises the shared-memory limit
     const int grid = grid_for(p.num_tiles, 1);
