@@ -442,17 +442,11 @@ struct ArithOzaki {
       for (int k = 0; k < pc.kc; ++k) m = fmax(m, fabs(opb(pc, B, k, lane)));
       eb = exp_above(m);
     }
-    int erow[2][2], fb[4], fcol[4][2];
+    int erow[2][2];
 #pragma unroll
     for (int mt = 0; mt < 2; ++mt)
 #pragma unroll
       for (int h = 0; h < 2; ++h) erow[mt][h] = __shfl_sync(FULL, ea, 16 * mt + gid + 8 * h);
-#pragma unroll
-    for (int nt = 0; nt < 4; ++nt) {
-      fb[nt] = __shfl_sync(FULL, eb, 8 * nt + gid);
-#pragma unroll
-      for (int h = 0; h < 2; ++h) fcol[nt][h] = __shfl_sync(FULL, eb, 8 * nt + 2 * tig + h);
-    }
     const int MT = (pc.M + 15) >> 4, NT = (pc.N + 7) >> 3;
     // A digits: [mt][register][slice]
     uint32_t ad[2][4][S];
@@ -475,9 +469,15 @@ struct ArithOzaki {
           }
         }
       }
+    // Column tiles in a rolled loop: the body (45 digit MMAs per row tile at
+    // 9 slices) is kept once in the instruction stream, which a 4-way unrolled
+    // copy overflowed; the accumulator is written through a static select.
+#pragma unroll 1
+    for (int nt = 0; nt < NT; ++nt) {
+      const int fb_nt = __shfl_sync(FULL, eb, 8 * nt + gid);
+      int fcol_nt[2];
 #pragma unroll
-    for (int nt = 0; nt < 4; ++nt) {
-      if (nt >= NT) continue;
+      for (int h = 0; h < 2; ++h) fcol_nt[h] = __shfl_sync(FULL, eb, 8 * nt + 2 * tig + h);
       // B digits of this column tile: [register][slice]
       uint32_t bd[2][S];
       const int col = 8 * nt + gid;
@@ -490,7 +490,7 @@ struct ArithOzaki {
           for (int w = 0; w < 4; ++w) {
             const int k = 4 * tig + 16 * rg + w;
             if (k < pc.kc) {
-              put_digits<S>(bd[rg], opb(pc, B, k, col), fb[nt], w);
+              put_digits<S>(bd[rg], opb(pc, B, k, col), fb_nt, w);
             }
           }
         }
@@ -516,12 +516,17 @@ struct ArithOzaki {
           for (int q = 0; q < 4; ++q) F[q] = fma(F[q], 0.0078125, (double)D[q]);
         }
         // sum = 2^-14 F; element scale 2^(e_i + f_j)
+        double pv[4];
 #pragma unroll
-        for (int q = 0; q < 4; ++q) {
-          const int e = erow[mt][q >> 1] + fcol[nt][q & 1] - 14;
-          const double pv = ldexp(F[q], e);
-          double &c = acc[(mt * 4 + nt) * 4 + q];
-          c = pc.alpha == 1.0 ? c + pv : fma(pc.alpha, pv, c);
+        for (int q = 0; q < 4; ++q) pv[q] = ldexp(F[q], erow[mt][q >> 1] + fcol_nt[q & 1] - 14);
+#pragma unroll
+        for (int n2 = 0; n2 < 4; ++n2) {
+          if (n2 != nt) continue;
+#pragma unroll
+          for (int q = 0; q < 4; ++q) {
+            double &c = acc[(mt * 4 + n2) * 4 + q];
+            c = pc.alpha == 1.0 ? c + pv[q] : fma(pc.alpha, pv[q], c);
+          }
         }
       }
     }
