@@ -460,7 +460,7 @@ struct ArithOzaki {
         const int kb = 4 * tig + 16 * (rg >> 1);
         if (mt < MT && row < pc.M) {
           const int st = A.start(row);
-#pragma unroll
+#pragma unroll 1
           for (int w = 0; w < 4; ++w) {
             const int k = kb + w;
             if (k < pc.kc) {
@@ -486,7 +486,7 @@ struct ArithOzaki {
 #pragma unroll
         for (int s = 0; s < S; ++s) bd[rg][s] = 0u;
         if (col < pc.N) {
-#pragma unroll
+#pragma unroll 1
           for (int w = 0; w < 4; ++w) {
             const int k = 4 * tig + 16 * rg + w;
             if (k < pc.kc) {
