@@ -4,8 +4,8 @@
 // accumulate into the same C block (C += A_p B_p).
 //
 // Work unit: one run (maximal group of consecutive entries naming the same C)
-// and one 32 x 32 tile of its C block.  The CTA (128 threads, 2 x 4 outputs
-// each) loads the C tile once, applies the run's products in array order with
+// and one 32 x 32 tile of its C block.  The CTA (64 threads, 4 x 4 outputs
+// each, six CTAs per SM) loads the C tile once, applies the run's products in array order with
 // the C tile held in registers (C = alpha_p A_p op(B_p) + beta_p C), and writes
 // it once -- the owner-computes rule that keeps shared C blocks race-free and
 // the result deterministic without atomics.  A and op(B) arrive in 32 x 32
@@ -29,7 +29,7 @@ namespace ls {
 
 namespace {
 
-constexpr int DR_THREADS = 128;
+constexpr int DR_THREADS = 64;
 constexpr int DR_T = 32;       // C tile edge and K slab
 constexpr int DR_P = 34;       // padded pitch (doubles) of the staged slabs
 constexpr int DR_STAGE = 2 * DR_T * DR_P;  // doubles per stage: A^T and B
@@ -85,12 +85,12 @@ struct DCursor {
   int t, p, k;
 };
 
-__global__ void __launch_bounds__(DR_THREADS, 4)
+__global__ void __launch_bounds__(DR_THREADS, 6)
     k_dgemm_runs(const LibShalom_dgemm_entry *entries, const unsigned *n_runs_p,
                  const unsigned *run_first, const unsigned *run_len) {
   __shared__ __align__(16) double stage[2][DR_STAGE];
   const int tid = threadIdx.x;
-  const int tx = tid & 7, ty = tid >> 3;  // outputs: rows 2ty, 2ty+1; cols 4tx..4tx+3
+  const int tx = tid & 7, ty = tid >> 3;  // outputs: rows 4ty..4ty+3; cols 4tx..4tx+3
   const long n_runs = (long)*n_runs_p;
 
   auto tiles_of = [&](const LibShalom_dgemm_entry &e) {
@@ -157,7 +157,7 @@ __global__ void __launch_bounds__(DR_THREADS, 4)
   load(cur, 0);
   cp_commit();
 
-  double c[2][4], acc[2][4];
+  double c[4][4], acc[4][4];
   int buf = 0;
   for (;;) {
     const unsigned f = run_first[cur.r];
@@ -165,21 +165,21 @@ __global__ void __launch_bounds__(DR_THREADS, 4)
     const DJob jb = djob(entries[f + cur.p]);
     const int tiles_n = (e0.N + DR_T - 1) / DR_T;
     const int m0 = (cur.t / tiles_n) * DR_T, n0 = (cur.t % tiles_n) * DR_T;
-    double *Crow0 = entries[f].C + (long)(m0 + 2 * ty) * (e0.ldc > 0 ? e0.ldc : e0.N) + n0 + 4 * tx;
+    double *Crow0 = entries[f].C + (long)(m0 + 4 * ty) * (e0.ldc > 0 ? e0.ldc : e0.N) + n0 + 4 * tx;
     const int ldc = e0.ldc > 0 ? e0.ldc : e0.N;
     if (cur.p == 0 && cur.k == 0) {
       // new C tile: load it (the run's first beta decides whether it is read)
 #pragma unroll
-      for (int i = 0; i < 2; ++i)
+      for (int i = 0; i < 4; ++i)
 #pragma unroll
         for (int j = 0; j < 4; ++j) {
-          const bool ok = m0 + 2 * ty + i < e0.M && n0 + 4 * tx + j < e0.N;
+          const bool ok = m0 + 4 * ty + i < e0.M && n0 + 4 * tx + j < e0.N;
           c[i][j] = ok ? Crow0[(long)i * ldc + j] : 0.0;
         }
     }
     if (cur.k == 0) {
 #pragma unroll
-      for (int i = 0; i < 2; ++i)
+      for (int i = 0; i < 4; ++i)
 #pragma unroll
         for (int j = 0; j < 4; ++j) acc[i][j] = 0.0;
     }
@@ -192,20 +192,21 @@ __global__ void __launch_bounds__(DR_THREADS, 4)
     const double *Bs = stage[buf] + DR_T * DR_P;
     const int kcnt = min(DR_T, jb.K - cur.k * DR_T);
     for (int k = 0; k < kcnt; ++k) {
-      const double2 a = *reinterpret_cast<const double2 *>(As + k * DR_P + 2 * ty);
+      const double2 a0 = *reinterpret_cast<const double2 *>(As + k * DR_P + 4 * ty);
+      const double2 a1 = *reinterpret_cast<const double2 *>(As + k * DR_P + 4 * ty + 2);
       const double2 b0 = *reinterpret_cast<const double2 *>(Bs + k * DR_P + 4 * tx);
       const double2 b1 = *reinterpret_cast<const double2 *>(Bs + k * DR_P + 4 * tx + 2);
-      const double av[2] = {a.x, a.y};
+      const double av[4] = {a0.x, a0.y, a1.x, a1.y};
       const double bv[4] = {b0.x, b0.y, b1.x, b1.y};
 #pragma unroll
-      for (int i = 0; i < 2; ++i)
+      for (int i = 0; i < 4; ++i)
 #pragma unroll
         for (int j = 0; j < 4; ++j) acc[i][j] = __fma_rn(av[i], bv[j], acc[i][j]);
     }
     const bool product_done = cur.k + 1 >= max(1, (jb.K + DR_T - 1) / DR_T);
     if (product_done) {
 #pragma unroll
-      for (int i = 0; i < 2; ++i)
+      for (int i = 0; i < 4; ++i)
 #pragma unroll
         for (int j = 0; j < 4; ++j) {
           const double v = jb.alpha * acc[i][j];
@@ -214,10 +215,10 @@ __global__ void __launch_bounds__(DR_THREADS, 4)
       if (cur.p + 1 == (int)run_len[cur.r]) {
         // run complete for this tile: write it
 #pragma unroll
-        for (int i = 0; i < 2; ++i)
+        for (int i = 0; i < 4; ++i)
 #pragma unroll
           for (int j = 0; j < 4; ++j)
-            if (m0 + 2 * ty + i < e0.M && n0 + 4 * tx + j < e0.N) Crow0[(long)i * ldc + j] = c[i][j];
+            if (m0 + 4 * ty + i < e0.M && n0 + 4 * tx + j < e0.N) Crow0[(long)i * ldc + j] = c[i][j];
       }
     }
     __syncthreads();  // everyone is done with this buffer before it is refilled
@@ -245,7 +246,7 @@ int run_dgemm_runs(const LibShalom_dgemm_entry *entries, long count) {
   const int pgrid = (int)std::max(1L, std::min(cdiv(count, 256), (long)st.num_sms * 8));
   k_drun_plan<<<pgrid, 256, 0, st.stream>>>(entries, count, pl);
   LS_CUDA_TRY(cudaGetLastError());
-  const int per_sm = occupancy_of((const void *)k_dgemm_runs, DR_THREADS, 0, 4);
+  const int per_sm = occupancy_of((const void *)k_dgemm_runs, DR_THREADS, 0, 6);
   const int grid = grid_for(cdiv(count, 1), per_sm);
   k_dgemm_runs<<<grid, DR_THREADS, 0, st.stream>>>(entries, pl.n_runs, pl.run_first, pl.run_len);
   LS_CUDA_TRY(cudaGetLastError());
@@ -256,7 +257,7 @@ int run_dgemm_runs(const LibShalom_dgemm_entry *entries, long count) {
 int run_dgemm_runs_list(const LibShalom_dgemm_entry *entries, long count, const unsigned *n_runs,
                         const unsigned *run_first, const unsigned *run_len) {
   State &st = state();
-  const int per_sm = occupancy_of((const void *)k_dgemm_runs, DR_THREADS, 0, 4);
+  const int per_sm = occupancy_of((const void *)k_dgemm_runs, DR_THREADS, 0, 6);
   const int grid = grid_for(cdiv(count, 1), per_sm);
   k_dgemm_runs<<<grid, DR_THREADS, 0, st.stream>>>(entries, n_runs, run_first, run_len);
   LS_CUDA_TRY(cudaGetLastError());
