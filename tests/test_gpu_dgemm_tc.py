@@ -148,3 +148,50 @@ def test_ozaki_error_shrinks_with_slices(slices, method_reset):
     ls.dgemm_batched(dE, count)
     err = max(run_errors(to_host(dC), ref, blocks))
     assert err <= 2.0 ** (-7 * slices) * 2000, err
+
+
+@pytest.mark.parametrize("transb", [0, 1], ids=["nn", "nt"])
+def test_fma_runs_bitexact_with_kseq_oracle(transb, method_reset):
+    """The FP64 FMA grouped kernel (LIBSHALOM_DGEMM_FMA) with alpha = 1, beta =
+    0 and one product per C: every element is one fused multiply-add chain
+    over k in increasing order, bit for bit the oracle's k-sequential
+    restatement, across single and multi-tile blocks, K below, at and above
+    one 32-k slab, and every residue of M and N modulo the 4 x 4 thread
+    tile."""
+    import torch
+    shapes = [(5, 13, 1), (13, 5, 7), (32, 32, 31), (32, 32, 32), (33, 40, 33), (40, 33, 70),
+              (6, 7, 64), (17, 30, 95)]
+    rng = np.random.default_rng(4242 + transb)
+    _, ddt = ls.entry_dtypes()
+    ent = np.zeros(len(shapes), ddt)
+    As, Bs, offs = [], [], []
+    oa = ob = oc = 0
+    for i, (M, N, K) in enumerate(shapes):
+        A = rng.standard_normal((M, K))
+        B = rng.standard_normal((N, K) if transb else (K, N))
+        As.append(A.ravel())
+        Bs.append(B.ravel())
+        offs.append((oa, ob, oc))
+        oa += A.size
+        ob += B.size
+        oc += M * N
+    dA = to_dev(np.concatenate(As))
+    dB = to_dev(np.concatenate(Bs))
+    dC = torch.full((oc,), float("nan"), dtype=torch.float64, device="cuda")
+    for i, (M, N, K) in enumerate(shapes):
+        a0, b0, c0 = offs[i]
+        ent[i]["A"] = dA.data_ptr() + 8 * a0
+        ent[i]["B"] = dB.data_ptr() + 8 * b0
+        ent[i]["C"] = dC.data_ptr() + 8 * c0
+        ent[i]["M"], ent[i]["N"], ent[i]["K"], ent[i]["transb"] = M, N, K, transb
+        ent[i]["alpha"], ent[i]["beta"] = 1.0, 0.0
+    dE = torch.from_numpy(ent.view(np.uint8)).cuda()
+    ls.set_dgemm_method(ls.DGEMM_FMA, 0)
+    ls.dgemm_batched(dE, len(shapes))
+    got = to_host(dC)
+    for i, (M, N, K) in enumerate(shapes):
+        a0, b0, c0 = offs[i]
+        A = As[i].reshape(M, K)
+        B = Bs[i].reshape((N, K) if transb else (K, N))
+        ref = orc.dgemm_kseq(A, B, transb)
+        assert np.array_equal(got[c0:c0 + M * N].reshape(M, N), ref), (M, N, K)

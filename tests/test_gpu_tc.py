@@ -104,10 +104,12 @@ def test_tc_batch_every_gemm_and_nothing_past_c(M, N, K, transb, mode_setter):
 @pytest.mark.parametrize("mode", [ls.PREC_BF16X6, ls.PREC_BF16X3])
 @pytest.mark.parametrize("transb", [0, 1])
 @pytest.mark.parametrize("M,N,K", [(100, 1, 40), (130, 16, 33), (96, 17, 300), (200, 32, 64),
-                                   (70, 29, 700)])
+                                   (70, 29, 700), (96, 48, 520), (130, 64, 300), (70, 65, 300)])
 def test_tc_narrow_tiles(M, N, K, transb, mode, mode_setter, staging):
     """Tiles of at most 32 columns, one GEMM per tile (MMA N of 16 or 32),
-    short K and the long-K register fold."""
+    short K and the long-K register fold; with long K, tiles of 48 and 64
+    columns take the narrow fold (one 32-column block per epilogue warp) and
+    80 columns the full one."""
     count = 5
     A, B, _, C = _strided(mode, transb, M, N, K, count, seed=M + 3 * N + K + transb)
     for g in range(count):
