@@ -615,11 +615,11 @@ struct WsArgs {
 __device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
   asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(ptx::smem_u32(bar)) : "memory");
 }
-// Arrival that publishes no memory: the default (release) arrive first waits
-// for this thread's earlier global stores to be acknowledged, which costs an
-// epilogue thousands of cycles per tile.  For arrivals that only say "done
-// reading" (TMEM read back and waited for, a queue slot copied into
-// registers) nothing has to be published.
+// Arrival that publishes no memory.  The default arrive has release
+// semantics: it orders this thread's earlier memory operations, the
+// epilogue's global C stores included, before the arrival.  Arrivals that
+// only say "done reading" (TMEM read back and waited for, a queue slot
+// copied into registers) have nothing to publish.
 __device__ __forceinline__ void mbar_arrive_relaxed(uint64_t *bar) {
   asm volatile("mbarrier.arrive.relaxed.cta.shared::cta.b64 _, [%0];" ::"r"(ptx::smem_u32(bar))
                : "memory");
@@ -646,8 +646,8 @@ __device__ __forceinline__ void tma_load_3d(uint32_t dst, const CUtensorMap *map
 // would make the caller save its live registers to local memory around every
 // wait.
 __device__ __forceinline__ bool ws_wait_slow(uint64_t *bar, uint32_t parity,
-                                          volatile int *abort_flag, unsigned *err,
-                                          uint32_t limit) {
+                                             volatile int *abort_flag, unsigned *err,
+                                             uint32_t limit) {
   const uint64_t t0 = ptx::globaltimer_ns();
   for (uint32_t it = 0; it < limit; ++it) {
     if (ptx::mbar_try_wait_suspend(bar, parity, 1000)) return true;
